@@ -1,0 +1,340 @@
+"""Benchmark of the B200 null-geodesic tracer (one JSON line on rank 0).
+
+    python bench.py [--gpus N] [--steps K] [--warmup W] [--impl b200|reference]
+
+Workload (one step): the 1920x1080 Kerr a*=+0.9 and Kerr-Newman a*=-0.7 q=0.4
+pair, camera r = 20, inclination 80 deg, FOV 45 deg, disk + hot spots, bloom +
+tonemap, 8 frames each with diskTime = k/7: 16 full frames through
+launchRenderPipeline's two halves (bhRenderAccum + bhPostProcess), plain FP32
+RK4, balanced preset.  Metric: Mrays/s (one primary ray per pixel) over the
+whole job, plus frame ms.
+
+  value      device-resident throughput: per step an L2 flush (256 MiB memset,
+             outside the timed events), then the 16 frames timed with CUDA
+             events on the launch stream; max over ranks.
+  e2e        the reference-facing call: launchRenderPipeline with RenderParams
+             from the host and the RGBA8 frame copied back to pinned host memory
+             inside the timed region.
+  roofline   the tracing kernel (dominant): algorithmic FLOPs / its event time
+             against the measured FP32 FMA peak.  Algorithmic FLOPs follow the
+             reference's work on the same inputs: RK4 steps x 420 (Kerr family)
+             or x 115 (spherical), + 500 per contributing disk sub-sample
+             + 250 per escaped ray, counted by the CPU oracle on a pixel sample
+             of every frame (the census in the CPU-baseline leg).
+  cpu_baseline  the reference's own tracer (src/trace.cuh built as host code,
+             oracle/_ref) on the host cores, on a bounded pixel sample.
+
+Multi-GPU: one process per GPU (torchrun); every rank renders its own 16-frame
+batch (frames offset in animation time), no collective on the data path
+("scaling": "weak"); timing is the max over ranks.
+"""
+import argparse
+import json
+import os
+import subprocess
+import sys
+import threading
+import time
+
+import numpy as np
+
+ROOT = os.path.dirname(os.path.abspath(__file__))
+sys.path.insert(0, os.path.join(ROOT, "black-hole_b200"))
+
+C_STEP_KERR, C_STEP_SPH, C_DISK, C_BG = 420.0, 115.0, 500.0, 250.0
+FRAMES_PER_SCENE = 8
+W, H = 1920, 1080
+L2_FLUSH_BYTES = 256 << 20
+RAY_BYTES = 160   # RenderParams per frame, passed by value to the launch
+
+
+def parse():
+    ap = argparse.ArgumentParser()
+    ap.add_argument("--gpus", type=int, default=1)
+    ap.add_argument("--steps", type=int, default=5)
+    ap.add_argument("--warmup", type=int, default=3)
+    ap.add_argument("--impl", default="b200", choices=["b200", "reference"])
+    ap.add_argument("--no-cpu-baseline", action="store_true")
+    ap.add_argument("--baseline-seconds", type=float, default=12.0)
+    return ap.parse_args()
+
+
+def workload(derive, rank=0):
+    from bhrt import scenes
+    frames = scenes.kerr_pair_1080(derive, W, H, FRAMES_PER_SCENE)
+    for P in frames:
+        P.diskTime = P.diskTime + float(rank)   # weak scaling: distinct frames per rank
+    return frames
+
+
+# ---------------------------------------------------------------------------
+# clocks during the timed region
+# ---------------------------------------------------------------------------
+class ClockSampler:
+    Q = ("clocks.sm,clocks.max.sm,power.draw,clocks_event_reasons.hw_slowdown,"
+         "clocks_event_reasons.hw_thermal_slowdown,clocks_event_reasons.sw_thermal_slowdown,"
+         "clocks_event_reasons.sw_power_cap")
+
+    def __init__(self, index):
+        self.index, self.rows, self.proc = index, [], None
+
+    def start(self):
+        try:
+            self.proc = subprocess.Popen(["nvidia-smi", "-i", str(self.index), f"--query-gpu={self.Q}",
+                                          "--format=csv,noheader,nounits", "-lms", "200"],
+                                         stdout=subprocess.PIPE, stderr=subprocess.DEVNULL, text=True)
+            self.thread = threading.Thread(target=self._read, daemon=True)
+            self.thread.start()
+        except OSError:
+            self.proc = None
+
+    def _read(self):
+        for line in self.proc.stdout:
+            parts = [p.strip() for p in line.split(",")]
+            if len(parts) == 7:
+                self.rows.append(parts)
+
+    def stop(self):
+        if self.proc is None:
+            return {"sm_mhz": None, "sm_max_mhz": None, "reasons": ["nvidia-smi unavailable"]}
+        self.proc.terminate()
+        try:
+            self.proc.wait(timeout=5)
+        except subprocess.TimeoutExpired:
+            self.proc.kill()
+        sm = [float(r[0]) for r in self.rows if r[0].replace(".", "").isdigit()]
+        mx = [float(r[1]) for r in self.rows if r[1].replace(".", "").isdigit()]
+        names = ["hw_slowdown", "hw_thermal_slowdown", "sw_thermal_slowdown", "sw_power_cap"]
+        reasons = sorted({names[i] for r in self.rows for i in range(4) if r[3 + i] == "Active"})
+        return {"sm_mhz": float(np.median(sm)) if sm else None, "sm_max_mhz": max(mx) if mx else None,
+                "reasons": reasons, "samples": len(self.rows)}
+
+
+# ---------------------------------------------------------------------------
+# CPU-baseline leg: the reference's tracer on the host cores + its work census
+# ---------------------------------------------------------------------------
+def sample_pixels(frame_idx, stride, W_, H_):
+    ys = np.arange((frame_idx * 7) % stride, H_, stride)
+    xs = np.arange((frame_idx * 13) % stride, W_, stride)
+    yy, xx = np.meshgrid(ys, xs, indexing="ij")
+    return (yy * W_ + xx).ravel().astype(np.int32)
+
+
+def cpu_baseline_leg(frames, seconds):
+    """Time the reference tracer on a pixel sample of the workload, and count
+    the reference's algorithmic work (RK4 steps, disk sub-samples, escapes) on
+    the same frames for the FLOP accounting."""
+    sys.path.insert(0, os.path.join(ROOT, "oracle"))
+    import oracle as orc
+    cores = os.cpu_count() or 1
+    # census: restated oracle (bit-exact with the reference) on a 1/24^2 sample of every frame
+    port = orc.Oracle()
+    census = []
+    for k, P in enumerate(frames):
+        rec = port.trace_pixels(P, sample_pixels(k, 24, P.width, P.height))
+        kerr = P.model in (2, 3)
+        flops = (rec["steps"].astype(np.float64) * (C_STEP_KERR if kerr else C_STEP_SPH)
+                 + rec["diskSamples"] * C_DISK + (rec["outcome"] == 1) * C_BG)
+        census.append({"flops_per_ray": float(flops.mean()), "steps_per_ray": float(rec["steps"].mean()),
+                       "disk_per_ray": float(rec["diskSamples"].mean())})
+    # timing: the reference's own build when present, else the restated port
+    kind = "reference" if orc.RefHost.available() else "port"
+    ref = orc.RefHost() if kind == "reference" else None
+    done, t0, chunks = 0, time.perf_counter(), 0
+    while True:
+        k = chunks % len(frames)
+        pix = sample_pixels(k + 31 * (chunks // len(frames)), 16, frames[k].width, frames[k].height)
+        if ref is not None:
+            ref.render_pixels(frames[k], pix, threads=cores)
+        else:
+            port.trace_pixels(frames[k], pix, threads=cores)
+        done += len(pix)
+        chunks += 1
+        if time.perf_counter() - t0 >= seconds and chunks >= len(frames):
+            break
+    el = time.perf_counter() - t0
+    return {"value": done / el / 1e6, "unit": "Mrays/s", "cores": cores, "kind": kind,
+            "sample": f"{done} rays: 1/256 strided pixel samples of the 16 workload frames, "
+                      f"{el:.1f} s on {cores} threads"}, census
+
+
+# ---------------------------------------------------------------------------
+# our arm
+# ---------------------------------------------------------------------------
+def run_b200(args, rank, world, local_rank):
+    import torch
+    import torch.distributed as dist
+    from bhrt import lib
+    from bhrt.device import Frame, measure_fp32_peak
+    import ctypes as C
+
+    torch.cuda.set_device(local_rank)
+    dev = torch.device("cuda", local_rank)
+    frames = workload(lib.derive, rank)
+    f = Frame(W, H, device=dev)
+    L = lib.load()
+    stream = torch.cuda.current_stream()
+    sp = C.c_void_p(stream.cuda_stream)
+    ptr = lambda t: C.c_void_p(t.data_ptr())  # noqa: E731
+    flush = torch.empty(L2_FLUSH_BYTES, dtype=torch.uint8, device=dev)
+    peak = measure_fp32_peak()
+
+    def step(evs=None):
+        for i, P in enumerate(frames):
+            if evs is not None:
+                evs[i][0].record(stream)
+            lib.check(L.bhRenderAccum(ptr(f.accum), C.byref(P), 0, sp), "bhRenderAccum")
+            if evs is not None:
+                evs[i][1].record(stream)
+            lib.check(L.bhPostProcess(ptr(f.out), ptr(f.accum), ptr(f.bloomA), ptr(f.bloomB), C.byref(P), sp),
+                      "bhPostProcess")
+            if evs is not None:
+                evs[i][2].record(stream)
+
+    for _ in range(args.warmup):
+        step()
+    torch.cuda.synchronize()
+
+    nF = len(frames)
+    evs = [[[torch.cuda.Event(enable_timing=True) for _ in range(3)] for _ in range(nF)]
+           for _ in range(args.steps)]
+    clocks = ClockSampler(local_rank)
+    if world > 1:
+        dist.barrier()
+    torch.cuda.synchronize()
+    clocks.start()
+    for s in range(args.steps):
+        flush.zero_()
+        step(evs[s])
+    torch.cuda.synchronize()
+    if world > 1:
+        dist.barrier()
+    clk = clocks.stop()
+    trace_ms = np.array([[evs[s][i][0].elapsed_time(evs[s][i][1]) for i in range(nF)] for s in range(args.steps)])
+    post_ms = np.array([[evs[s][i][1].elapsed_time(evs[s][i][2]) for i in range(nF)] for s in range(args.steps)])
+    step_ms = (trace_ms + post_ms).sum(axis=1)
+    total_ms = float(step_ms.sum())
+
+    # e2e: the reference-facing call, params from the host, RGBA8 back to pinned host memory
+    host = torch.empty((H, W, 4), dtype=torch.uint8, pin_memory=True)
+    e2 = [(torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)) for _ in range(args.steps)]
+    for s in range(-1, args.steps):
+        flush.zero_()
+        if s >= 0:
+            e2[s][0].record(stream)
+        for P in frames:
+            lib.check(L.launchRenderPipeline(ptr(f.out), ptr(f.accum), ptr(f.bloomA), ptr(f.bloomB),
+                                             C.byref(P), sp), "launchRenderPipeline")
+            host.copy_(f.out, non_blocking=True)
+        if s >= 0:
+            e2[s][1].record(stream)
+    torch.cuda.synchronize()
+    e2e_ms = float(sum(a.elapsed_time(b) for a, b in e2))
+
+    t = torch.tensor([total_ms, e2e_ms, float(trace_ms.sum())], dtype=torch.float64, device=dev)
+    if world > 1:
+        dist.all_reduce(t, op=dist.ReduceOp.MAX)
+    total_ms, e2e_ms, trace_total = t.tolist()
+    rays_step = nF * W * H
+    out = {
+        "metric": "Mrays/s (plain FP32 RK4, 1920x1080 Kerr/Kerr-Newman pair, 16 frames)",
+        "value": world * rays_step * args.steps / (total_ms * 1e-3) / 1e6,
+        "unit": "Mrays/s",
+        "n_gpus": world, "steps": args.steps, "warmup": args.warmup,
+        "ms_per_step": total_ms / args.steps,
+        "frame_ms": float(np.median(trace_ms + post_ms)),
+        "trace_ms_per_frame": float(np.median(trace_ms)),
+        "post_ms_per_frame": float(np.median(post_ms)),
+        "higher_is_better": True, "scaling": "weak", "vs_baseline": None,
+        "dtype": "f32", "data": "synthetic (procedural scenes of the named configuration)",
+        "config": {"workload": "kerr_a0.9+kn_a-0.7_q0.4_1920x1080_8frames_each_bloom",
+                   "frames_per_step": nF, "width": W, "height": H, "preset": "balanced dPhi=0.012 maxSteps=2000",
+                   "camera": "r=20 rs, inclination 80 deg, FOV 45 deg", "precision": "fp32",
+                   "l2": "flushed (256 MiB memset) before every timed step",
+                   "parallelism": f"replicas x{world} (frames per rank, no collective)"},
+        "e2e": {"value": world * rays_step * args.steps / (e2e_ms * 1e-3) / 1e6, "unit": "Mrays/s",
+                "h2d_bytes_per_step": nF * RAY_BYTES, "d2h_bytes_per_step": nF * W * H * 4},
+        "gpu_launches": args.steps * nF * 3,
+        "clocks": clk,
+        "fp32_peak_tflops_measured": peak,
+    }
+    return out, trace_total
+
+
+def main():
+    args = parse()
+    rank = int(os.environ.get("RANK", "0"))
+    world = int(os.environ.get("WORLD_SIZE", "1"))
+    local_rank = int(os.environ.get("LOCAL_RANK", "0"))
+
+    if args.impl == "reference":
+        if rank != 0:
+            return
+        return run_reference(args)
+
+    import torch
+    import torch.distributed as dist
+    if world > 1:
+        from datetime import timedelta
+        dist.init_process_group("nccl", timeout=timedelta(seconds=120))
+    out, trace_total_ms = run_b200(args, rank, world, local_rank)
+    if rank == 0:
+        from bhrt import lib
+        frames = workload(lib.derive, 0)
+        if not args.no_cpu_baseline:
+            base, census = cpu_baseline_leg(frames, args.baseline_seconds)
+            flops_frame = [c["flops_per_ray"] * W * H for c in census]
+            flops_step = float(sum(flops_frame))
+            achieved = flops_step * args.steps / (trace_total_ms * 1e-3) / 1e12
+            peak = out["fp32_peak_tflops_measured"]
+            out["roofline"] = {"bound": "fp32", "achieved": achieved, "peak": peak, "unit": "TFLOP/s",
+                               "frac": achieved / peak if peak else None, "traffic": None,
+                               "peak_source": "measured FP32 FMA microbenchmark (bhMeasureFp32Peak), same run",
+                               "flops_per_frame": flops_step / len(frames),
+                               "steps_per_ray": float(np.mean([c["steps_per_ray"] for c in census]))}
+            out["cpu_baseline"] = base
+        print(json.dumps(out))
+    if world > 1:
+        dist.barrier()
+        dist.destroy_process_group()
+
+
+def run_reference(args):
+    sys.path.insert(0, os.path.join(ROOT, "oracle"))
+    import oracle as orc
+    from bhrt import lib
+    frames = workload(lib.derive, 0)
+    cores = os.cpu_count() or 1
+    kind = "reference" if orc.RefHost.available() else "port"
+    impl = orc.RefHost() if kind == "reference" else orc.Oracle()
+
+    def one(k):
+        P = frames[k % len(frames)]
+        pix = sample_pixels(k, 6, P.width, P.height)
+        if kind == "reference":
+            impl.render_pixels(P, pix, threads=cores)
+        else:
+            impl.trace_pixels(P, pix, threads=cores)
+        return len(pix)
+
+    for k in range(args.warmup):
+        one(k)
+    t0 = time.perf_counter()
+    n = sum(one(args.warmup + k) for k in range(args.steps))
+    el = time.perf_counter() - t0
+    v = n / el / 1e6
+    out = {"impl": "reference",
+           "metric": "Mrays/s (plain FP32 RK4, 1920x1080 Kerr/Kerr-Newman pair, 16 frames)",
+           "value": v, "unit": "Mrays/s", "n_gpus": 1, "steps": args.steps, "warmup": args.warmup,
+           "ms_per_step": el * 1e3 / args.steps, "higher_is_better": True, "scaling": "weak",
+           "vs_baseline": None, "dtype": "f32", "data": "synthetic",
+           "config": {"workload": "kerr_a0.9+kn_a-0.7_q0.4_1920x1080_8frames_each_bloom",
+                      "sample": "each step traces a 1/6^2 strided pixel sample of one workload frame"},
+           "cpu_baseline": {"value": v, "unit": "Mrays/s", "cores": cores, "kind": kind,
+                            "sample": f"{n} rays over {args.steps} steps on {cores} threads"},
+           "e2e": {"value": v, "unit": "Mrays/s", "h2d_bytes_per_step": 0, "d2h_bytes_per_step": 0}}
+    print(json.dumps(out))
+
+
+if __name__ == "__main__":
+    main()

@@ -1,0 +1,28 @@
+#pragma once
+// ---------------------------------------------------------------------------
+// bh_internal.h -- declarations shared by the host C++ and the CUDA sources
+// of libbh.so (not part of the public C-ABI in include/).
+// ---------------------------------------------------------------------------
+#include <cuda_runtime_api.h>
+#include <vector_types.h>
+#include "bh_trace_params.h"
+
+#define BH_TRACE_BLOCK 128
+
+struct PostConsts
+{
+    float exposure, bloomStrength;
+    int bloomOn, swapRB;
+};
+
+// tracing: zero the ray counter, then one persistent launch (bh_trace.cu)
+cudaError_t bh_launch_trace(const TraceParams& P, int precision, bool stats, int blocksPerSm,
+                            cudaStream_t stream);
+
+// bloom + tonemap of an accumulation buffer (bh_post.cu); `hblur` holds the
+// horizontally blurred half-resolution image ((W+1)/2 x (H+1)/2 float4)
+cudaError_t bh_launch_post(uchar4* out, const float4* accum, float4* hblur, int W, int H,
+                           const PostConsts& pc, cudaStream_t stream);
+
+// FP32 FMA throughput probe (bh_peak.cu)
+double bh_measure_fp32_peak();

@@ -1,0 +1,66 @@
+// ---------------------------------------------------------------------------
+// bh_peak.cu -- measured FP32 FMA throughput of the current GPU.
+//
+// The tracer is FP32-bound, and no FP32 peak is published for this machine's
+// clocks, so the roofline denominator is measured: every thread runs eight
+// independent FMA chains (enough ILP to cover the FMA latency at full
+// occupancy), the grid fills every SM, and the launch is timed with CUDA
+// events after a warm-up.  FLOPs counted as 2 per FMA.
+// ---------------------------------------------------------------------------
+#include <cuda_runtime.h>
+#include "bh_internal.h"
+
+namespace {
+
+constexpr int kChains = 8;
+constexpr int kIters = 4096;
+
+__global__ void __launch_bounds__(256) fma_kernel(float* out, float a, float b)
+{
+    float x[kChains];
+#pragma unroll
+    for (int c = 0; c < kChains; ++c) x[c] = (float)(threadIdx.x + c) * 1e-3f;
+#pragma unroll 4
+    for (int i = 0; i < kIters; ++i)
+    {
+#pragma unroll
+        for (int c = 0; c < kChains; ++c) x[c] = fmaf(x[c], a, b);
+    }
+    float s = 0.f;
+#pragma unroll
+    for (int c = 0; c < kChains; ++c) s += x[c];
+    if (s == 1234.5678f) out[blockIdx.x] = s;   // keeps the chains live
+}
+
+}  // namespace
+
+double bh_measure_fp32_peak()
+{
+    int dev = 0, sms = 0;
+    if (cudaGetDevice(&dev) != cudaSuccess) return 0.0;
+    if (cudaDeviceGetAttribute(&sms, cudaDevAttrMultiProcessorCount, dev) != cudaSuccess) return 0.0;
+    float* out = nullptr;
+    const int blocks = sms * 8;
+    if (cudaMalloc(&out, blocks * sizeof(float)) != cudaSuccess) return 0.0;
+    cudaEvent_t e0, e1;
+    cudaEventCreate(&e0);
+    cudaEventCreate(&e1);
+    for (int w = 0; w < 3; ++w) fma_kernel<<<blocks, 256>>>(out, 0.999f, 1e-4f);
+    float best = 1e30f;
+    for (int rep = 0; rep < 5; ++rep)
+    {
+        cudaEventRecord(e0);
+        fma_kernel<<<blocks, 256>>>(out, 0.999f, 1e-4f);
+        cudaEventRecord(e1);
+        cudaEventSynchronize(e1);
+        float ms = 0.f;
+        cudaEventElapsedTime(&ms, e0, e1);
+        if (ms < best) best = ms;
+    }
+    cudaEventDestroy(e0);
+    cudaEventDestroy(e1);
+    cudaFree(out);
+    if (cudaGetLastError() != cudaSuccess) return 0.0;
+    const double flops = 2.0 * kChains * (double)kIters * 256.0 * blocks;
+    return flops / (best * 1e-3) / 1e12;
+}

@@ -1,0 +1,156 @@
+#pragma once
+/*
+ * bh_launch.h -- C-ABI of libbh.so, the B200 (sm_100a) null-geodesic tracer.
+ *
+ * The first two entry points are the drop-in boundary: same names, argument
+ * order, ownership and error behaviour as the reference launchers in
+ * src/black_hole_kernel.cu of Sqhh99/Black-hole.  Everything after them is
+ * an additive extension (probing, precision modes, batching, measurement).
+ *
+ * Conventions shared by every entry point
+ *  - All buffers are device pointers owned by the caller.
+ *  - Work is enqueued on `stream` and the call returns without
+ *    synchronising; the return value is the launch status
+ *    (cudaGetLastError after the enqueue), as in the reference.
+ *  - The caller's RenderParams is never modified: it is copied and the copy
+ *    is sanitised (bhSanitizeRenderParams) before use.
+ *  - Tracing kernels draw rays from a per-device work counter.  The library
+ *    allocates that small scratch block (4 KiB) once per device, on the
+ *    first call made on that device, and resets it on `stream` before every
+ *    launch; two launches that overlap on the GPU therefore must not share
+ *    a device.  Make the first call before any CUDA-graph capture begins.
+ */
+#include <cuda_runtime_api.h>
+#include <stdint.h>
+#include "bh_render_params.h"
+
+#ifdef __cplusplus
+#define BH_PARAMS_IN const RenderParams&
+extern "C" {
+#else
+#define BH_PARAMS_IN const RenderParams*
+#endif
+
+/* Metric families (reference metric.cuh:32-38). */
+enum { BH_SCHWARZSCHILD = 0, BH_REISSNER_NORDSTROM = 1, BH_KERR = 2, BH_KERR_NEWMAN = 3 };
+
+/* Arithmetic of the geodesic integration.
+ *  BH_PREC_FP32  : everything in FP32 (the reference's arithmetic).
+ *  BH_PREC_MIXED : FP32 stepping; FP64 for the conserved-quantity set-up at
+ *                  the camera, for the horizon/turning-point and escape
+ *                  decisions, and for bisection of equatorial disk crossings.
+ *  BH_PREC_FP64  : the whole integration in FP64 (GPU oracle). */
+enum { BH_PREC_FP32 = 0, BH_PREC_MIXED = 1, BH_PREC_FP64 = 2 };
+
+/* Derived black-hole quantities (reference metric.cuh:204-215; the two bool
+ * flags are ints here so the struct is plain C). */
+typedef struct BHDerived
+{
+    float a, Q;          /* code units: a = a* M (signed), Q = q M */
+    float rPlus, rMinus; /* horizons (0 when naked) */
+    float rPhoton;       /* photon sphere / co-rotating photon orbit */
+    float rErgo;         /* equatorial ergosphere radius */
+    float rIsco;         /* numeric innermost stable circular orbit */
+    int   clamped;       /* inputs had to be modified */
+    int   naked;         /* a*^2 + q^2 > 1 */
+} BHDerived;
+
+/* Per-ray record written by the probe entry points.  Field meanings follow
+ * the reference TraceResult (src/trace.cuh:418-428) and its test probe
+ * (tests/test_main.cu:63-69); the last group is added by this library. */
+typedef struct BHProbe
+{
+    int   outcome;      /* 0 captured (horizon), 1 escaped -- reference Probe.outcome */
+    int   cls;          /* 0 captured, 1 disk hit (trans < 0.5), 2 escaped */
+    int   steps;        /* integration steps taken (reference TraceResult.steps) */
+    int   diskSamples;  /* disk sub-samples that contributed emission */
+    float escDir[3];    /* deflected escape direction (unit) */
+    float trans;        /* remaining transmittance */
+    float accum[3];     /* disk radiance accumulated along the ray */
+    float maxHviol;     /* max |K| / (E^2 (r^2 + a^2)) along a rotating-metric ray */
+    float hdr[3];       /* linear HDR sample (accum + sky * trans) */
+    float diskR;        /* cylindrical radius where trans first fell below 0.5 (0 if never) */
+    float diskG;        /* emitter redshift factor g at that sub-sample */
+    float drift;        /* relative drift of the conserved quantity (Carter Q or Binet integral) */
+} BHProbe;
+
+/* ---- drop-in boundary (reference src/black_hole_kernel.cu) ------------- */
+
+/* Full-quality frame: one geodesic sample per pixel blended into `accum`
+ * (W*H float4, persistent across frames), half-resolution bloom through
+ * `bloomA` / `bloomB` (ceil(W/2)*ceil(H/2) float4 each; unused when bloom is
+ * off), then exposure, ACES, gamma and dither into `out` (W*H uchar4).
+ * Replaces launchRenderPipeline, reference src/black_hole_kernel.cu:108-134. */
+cudaError_t launchRenderPipeline(uchar4* out, float4* accum, float4* bloomA, float4* bloomB,
+                                 BH_PARAMS_IN p, cudaStream_t stream);
+
+/* Single pass: one centred sample per pixel straight to `out`; no
+ * accumulation, bloom forced off.
+ * Replaces launchRenderKernel, reference src/black_hole_kernel.cu:151-163. */
+cudaError_t launchRenderKernel(uchar4* out, BH_PARAMS_IN p, cudaStream_t stream);
+
+/* ---- host-side parameter handling (reference src/metric.cuh) ----------- */
+
+/* Clamp every field to a renderable value; returns 1 if anything changed.
+ * Replaces sanitizeRenderParams, reference src/metric.cuh:344-419. */
+int bhSanitizeRenderParams(RenderParams* p);
+
+/* Validate (clamp) M, a*, q for `model` in place and derive horizons,
+ * photon orbit, ergosphere and numeric ISCO into *out.
+ * Replaces bhValidateAndDerive, reference src/metric.cuh:257-329. */
+void bhValidateAndDerive(int model, float* M, float* aStar, float* q, int allowNaked,
+                         BHDerived* out);
+
+/* ---- extensions ------------------------------------------------------- */
+
+/* Trace the nx*ny grid of pixel-centre rays of the camera in `p` and write
+ * one BHProbe per ray (row-major).  The analogue of the reference's test
+ * probe kernel (tests/test_main.cu:71-89), with constraint monitoring on. */
+cudaError_t bhProbeGrid(BHProbe* out, BH_PARAMS_IN p, int nx, int ny, int precision,
+                        cudaStream_t stream);
+
+/* Trace `n` arbitrary unit directions (float3, device memory) from the
+ * camera position (reference tests/test_main.cu:91-98, batched). */
+cudaError_t bhProbeRays(BHProbe* out, const float3* dirs, int n, BH_PARAMS_IN p,
+                        int precision, cudaStream_t stream);
+
+/* Linear-HDR frame: one sample per pixel (the same jitter rule as the
+ * pipeline) into `hdr` (W*H float4, alpha = 1), no blending, no
+ * post-processing.  The sample of reference renderSampleHDR
+ * (src/trace.cuh:908-926) for every pixel. */
+cudaError_t bhRenderHDR(float4* hdr, BH_PARAMS_IN p, int precision, cudaStream_t stream);
+
+/* Pipeline with a selectable integration precision (BH_PREC_*).  With
+ * BH_PREC_FP32 it is launchRenderPipeline. */
+cudaError_t bhRenderPipelinePrec(uchar4* out, float4* accum, float4* bloomA, float4* bloomB,
+                                 BH_PARAMS_IN p, int precision, cudaStream_t stream);
+
+/* The tracing half of the pipeline: one sample per pixel blended into
+ * `accum` exactly as launchRenderPipeline does, without post-processing.
+ * launchRenderPipeline == bhRenderAccum + bhPostProcess on the same stream. */
+cudaError_t bhRenderAccum(float4* accum, BH_PARAMS_IN p, int precision, cudaStream_t stream);
+
+/* Post-processing alone (bloom + tonemap of an existing accumulation
+ * buffer): reference src/black_hole_kernel.cu:41-103. */
+cudaError_t bhPostProcess(uchar4* out, const float4* accum, float4* bloomA, float4* bloomB,
+                          BH_PARAMS_IN p, cudaStream_t stream);
+
+/* Work-distribution tuning of a metric family (0: Schwarzschild / RN,
+ * 1: Kerr / Kerr-Newman): a warp refills its idle lanes once at least
+ * `refillMin` (1..32) are idle; `blocksPerSm` CTAs of 128 threads stay
+ * resident per SM (0: as many as occupancy allows).  Returns 1 when applied,
+ * 0 when a value is out of range.  Process-wide; set by the autotuner. */
+int bhSetTuning(int family, int refillMin, int blocksPerSm);
+void bhGetTuning(int family, int* refillMin, int* blocksPerSm);
+
+/* Measured FP32 FMA throughput of the current device, in TFLOP/s, from a
+ * dependent-chain FMA kernel timed with CUDA events (blocking). */
+double bhMeasureFp32Peak(void);
+
+/* Library version / build string. */
+const char* bhVersion(void);
+
+#ifdef __cplusplus
+}
+#endif
+#undef BH_PARAMS_IN
