@@ -113,6 +113,7 @@ TraceParams frameParams(const RenderParams& P, int outMode, void* out)
     t.swapRB = P.swapRB;
     const Tuning& tu = gTune[(P.model == BH_KERR || P.model == BH_KERR_NEWMAN) ? 1 : 0];
     t.refillMin = tu.refillMin;
+    bh_fill_camera_frames(t);
     return t;
 }
 

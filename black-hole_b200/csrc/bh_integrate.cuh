@@ -2,10 +2,10 @@
 // ---------------------------------------------------------------------------
 // bh_integrate.cuh -- the two geodesic integrators as resumable ray objects.
 //
-// Each integrator is split into init() / step() / finish() so that a warp can
-// hold 32 independent rays in registers and refill any lane whose ray ended
-// (persistent-warp ray compaction, bh_trace.cu).  The arithmetic per step is
-// the reference's method (Sqhh99/Black-hole):
+// Each integrator is split into init() / advance() / result() so that a warp
+// can hold 32 independent rays in registers and refill any lane whose ray
+// ended (bh_trace.cu).  The arithmetic per step is the reference's method
+// (Sqhh99/Black-hole):
 //   SphRay   generalised Binet equation u'' = 3Mu^2 - 2Q^2u^3 - u, RK4 in the
 //            orbital angle with the adaptive step of src/trace.cuh:466-611
 //   KerrRay  Boyer-Lindquist Hamiltonian system (r, th, ph, p_r, p_th) with the
@@ -15,16 +15,20 @@
 // Termination tests and their order are the reference's, so step counts and
 // outcomes agree ray by ray except where floating-point rounding decides.
 //
-// R is the integration precision (float: the product path; double: the GPU
+// Initial data: the camera-frame part is precomputed on the host (CamFrame);
+// the per-ray remainder here uses exact (correctly rounded, uncontracted)
+// operations, so every ray starts from the reference's initial state bit for
+// bit.  R is the integration precision (float: product path; double: GPU
 // accuracy oracle).  Shading stays float in both.
 //
-// Arithmetic choices for R = float: divisions by state-dependent quantities
-// use one MUFU reciprocal each (shared where a quantity divides twice);
-// sin/cos of the polar angle use the polynomial sincos_polar (relative
-// accuracy at the poles); the ever-growing azimuth uses sincos_fast.  The
-// escape direction is rebuilt once per ray with the accurate library sincos.
-// sin/cos of theta at the end of a step are carried into the next step's
-// first right-hand side, the slow-light term and the Cartesian chord.
+// Arithmetic of the FP32 step: divisions by state-dependent quantities use one
+// MUFU reciprocal each; sin/cos of the polar angle at the start of a step come
+// from the polynomial sincos_polar (relative accuracy at poles and equator)
+// and are carried into the next step's first right-hand side, the slow-light
+// term and the Cartesian chord; the three RK4 stage angles th + delta use the
+// angle-addition formula from that anchored pair; the ever-growing azimuth
+// uses sincos_fast.  The escape direction is rebuilt once per ray with the
+// accurate library sincos.
 // ---------------------------------------------------------------------------
 #include "bh_shade.cuh"
 
@@ -38,6 +42,26 @@ struct RayResult
 };
 
 enum { RAY_SKIP = 0, RAY_LIVE = 1, RAY_DONE = 2 };
+
+// ---- exact single operations in either precision --------------------------------
+BH_DEV float xmul(float a, float b) { return __fmul_rn(a, b); }
+BH_DEV double xmul(double a, double b) { return __dmul_rn(a, b); }
+BH_DEV float xadd(float a, float b) { return __fadd_rn(a, b); }
+BH_DEV double xadd(double a, double b) { return __dadd_rn(a, b); }
+BH_DEV float xsub(float a, float b) { return __fsub_rn(a, b); }
+BH_DEV double xsub(double a, double b) { return __dsub_rn(a, b); }
+BH_DEV float xdiv(float a, float b) { return __fdiv_rn(a, b); }
+BH_DEV double xdiv(double a, double b) { return __ddiv_rn(a, b); }
+BH_DEV float xsqrt(float a) { return __fsqrt_rn(a); }
+BH_DEV double xsqrt(double a) { return __dsqrt_rn(a); }
+template <class R> BH_DEV R xdot(const R* e, vec3<R> d)
+{
+    return xadd(xadd(xmul(d.x, e[0]), xmul(d.y, e[1])), xmul(d.z, e[2]));
+}
+
+template <class R> BH_DEV const CamFrame<R>& frame_of(const TraceParams& P);
+template <> BH_DEV const CamFrame<float>& frame_of<float>(const TraceParams& P) { return P.cf; }
+template <> BH_DEV const CamFrame<double>& frame_of<double>(const TraceParams& P) { return P.cd; }
 
 BH_DEV f3 camera_ray(const TraceParams& P, float fx, float fy)
 {
@@ -57,34 +81,31 @@ BH_DEV float capture_radius(const TraceParams& P)
     return (P.rPlus > 1e-6f) ? P.rPlus : 0.05f * P.M;
 }
 
-// Static-observer tetrad at the camera -> photon E, Lz (reference
-// src/trace.cuh:213-247); accurate library functions.
-template <class R>
-BH_DEV void conserved_EL(vec3<R> o, vec3<R> dir, R M, R a, R Q, R& E, R& Lz)
+// sin/cos of th + delta from the anchored pair (s, c) of th.  FP32: angle
+// addition with the Taylor series of sin / cos delta to degree 7 / 6
+// (truncation < 4e-10 for |delta| <= 0.3; the adaptive step keeps a stage's
+// angular advance below 2.2 dPhi <= 0.22); larger deltas fall back to the
+// full polynomial.  FP64: the library sincos.
+BH_DEV void sincos_shift(float th, float s, float c, float delta, float& so, float& co)
 {
-    R r0 = sqrt_p(dot3(o, o));
-    if (r0 < R(1e-4f)) { E = R(1); Lz = R(0); return; }
-    R cth0 = min_p(max_p(o.y / r0, R(-1)), R(1));
-    R th0 = acos(cth0);
-    R ph0 = atan2(-o.z, o.x);
-    R s = sin(th0);
-    R sp, cp;
-    sincos(ph0, &sp, &cp);
-    R dpc = -dir.x * sp - dir.z * cp;
-    R s0 = max_p(s, R(1e-4f));
-    R s02 = s0 * s0;
-    R Sig0 = r0 * r0 + a * a * cth0 * cth0;
-    R m2r0 = R(2) * M * r0 - Q * Q;
-    R gtt = -(R(1) - m2r0 / max_p(Sig0, R(1e-8f)));
-    if (gtt > R(-1e-5f)) gtt = R(-1e-5f);
-    R gtp = -a * m2r0 * s02 / Sig0;
-    R gpp = (r0 * r0 + a * a + m2r0 * a * a * s02 / Sig0) * s02;
-    R A = R(1) / sqrt_p(max_p(gpp - gtp * gtp / gtt, R(1e-8f)));
-    R ptUp = R(1) / sqrt_p(-gtt) - dpc * A * gtp / gtt;
-    R pfUp = dpc * A;
-    E = -(gtt * ptUp + gtp * pfUp);
-    Lz = gtp * ptUp + gpp * pfUp;
-    if (!(E > R(1e-6f)) || !finite_p(E)) { E = R(1); Lz = R(0); }
+    if (fabsf(delta) > 0.3f)
+    {
+        sincos_polar(th + delta, so, co);
+        return;
+    }
+    float d2 = delta * delta;
+    float ps = fmaf(d2, -1.98412698412698413e-4f, 8.33333333333333333e-3f);
+    ps = fmaf(d2, ps, -1.66666666666666667e-1f);
+    float sd = fmaf(delta * d2, ps, delta);
+    float pc = fmaf(d2, -1.38888888888888889e-3f, 4.16666666666666667e-2f);
+    pc = fmaf(d2, pc, -0.5f);
+    float cd = fmaf(d2, pc, 1.f);
+    so = fmaf(s, cd, c * sd);
+    co = fmaf(c, cd, -(s * sd));
+}
+BH_DEV void sincos_shift(double th, double, double, double delta, double& so, double& co)
+{
+    sincos(th + delta, &so, &co);
 }
 
 // ===========================================================================
@@ -94,7 +115,7 @@ template <class R, bool STATS>
 struct SphRay
 {
     R u, du, phi, tFlight, invB;
-    R e1x, e1y, e1z, e2x, e2y, e2z;   // orbital-plane basis
+    R e2x, e2y, e2z;                  // in-plane unit vector normal to e1 (e1 is the camera's)
     R ud, dud, phid;                  // state of the last chord direction (deferred)
     float E, Lz;                      // photon constants for the disk emitter
     f3 prevPos, accum;
@@ -106,42 +127,50 @@ struct SphRay
 
     BH_DEV int init(const TraceParams& P, f3 dirf)
     {
-        const R M = (R)P.M, Qc = (R)P.Q;
-        vec3<R> c = widen<R>(tof3(P.camPos));
-        vec3<R> dir = widen<R>(dirf);
-        R Eph, Lph;
-        conserved_EL(c, dir, M, R(0), Qc, Eph, Lph);
-        E = (float)Eph; Lz = (float)Lph;
-
+        const CamFrame<R>& F = frame_of<R>(P);
+        const vec3<R> dir = widen<R>(dirf);
         horizon = escaped = haveDir = false;
         accum = v3(0.f, 0.f, 0.f);
         trans = 1.f;
         step = 0;
         tFlight = R(0);
         prevPos = tof3(P.camPos);
-        if (STATS) { tally.samples = 0; tally.hitR = 0.f; tally.hitG = 0.f; }
+        if (STATS) { tally.samples = 0; tally.hitR = 0.f; tally.hitG = 0.f; I0 = 0.0; }
 
-        R r0 = sqrt_p(dot3(c, c));
-        R ir0 = R(1) / r0;
-        e1x = c.x * ir0; e1y = c.y * ir0; e1z = c.z * ir0;
-        R ddr = dir.x * e1x + dir.y * e1y + dir.z * e1z;
-        R px = dir.x - e1x * ddr, py = dir.y - e1y * ddr, pz = dir.z - e1z * ddr;
-        R pl = sqrt_p(px * px + py * py + pz * pz);
+        // photon E, Lz (reference src/trace.cuh:213-247 with a = 0)
+        R Eph = R(1), Lph = R(0);
+        if (!F.camAtOrigin)
+        {
+            R dpc = xdot(F.ephS, dir);
+            R ptUp = xsub(F.rsqS, xdiv(xmul(xmul(dpc, F.AS), F.gtpS), F.gttS));
+            R pfUp = xmul(dpc, F.AS);
+            Eph = -xadd(xmul(F.gttS, ptUp), xmul(F.gtpS, pfUp));
+            Lph = xadd(xmul(F.gtpS, ptUp), xmul(F.gppS, pfUp));
+            if (!(Eph > R(1e-6f)) || !finite_p(Eph)) { Eph = R(1); Lph = R(0); }
+        }
+        E = (float)Eph; Lz = (float)Lph;
+
+        // orbital plane (reference src/trace.cuh:490-521)
+        R ddr = xdot(F.e1, dir);
+        R px = xsub(dir.x, xmul(F.e1[0], ddr));
+        R py = xsub(dir.y, xmul(F.e1[1], ddr));
+        R pz = xsub(dir.z, xmul(F.e1[2], ddr));
+        R pl = xsqrt(xadd(xadd(xmul(px, px), xmul(py, py)), xmul(pz, pz)));
         if (pl < R(1e-6f))
         {   // exactly radial ray (reference src/trace.cuh:447-459, 500-505)
-            horizon = (dir.x * c.x + dir.y * c.y + dir.z * c.z) < R(0);
+            const vec3<R> c = widen<R>(tof3(P.camPos));
+            horizon = xadd(xadd(xmul(dir.x, c.x), xmul(dir.y, c.y)), xmul(dir.z, c.z)) < R(0);
             escaped = !horizon;
             return RAY_DONE;
         }
-        R ipl = R(1) / pl;
-        e2x = px * ipl; e2y = py * ipl; e2z = pz * ipl;
-        R f0 = max_p(R(1) - R(2) * M / r0 + Qc * Qc / (r0 * r0), R(1e-6f));
-        R sf0 = sqrt_p(f0);
-        invB = R(1) / max_p(r0 * pl / sf0, R(1e-6f));
-        u = ir0;
-        du = -sf0 * ddr / (r0 * pl);
+        R ipl = xdiv(R(1), pl);
+        e2x = xmul(px, ipl); e2y = xmul(py, ipl); e2z = xmul(pz, ipl);
+        R bImpact = max_p(xdiv(xmul(F.r0, pl), F.sf0), R(1e-6f));
+        invB = rcp_p(bImpact);
+        u = F.u0;
+        du = xdiv(xmul(-F.sf0, ddr), xmul(F.r0, pl));
         phi = R(0);
-        if (STATS) I0 = binet(M, Qc * Qc, u, du);
+        if (STATS) I0 = binet((R)P.M, (R)P.Q * (R)P.Q, u, du);
         return RAY_LIVE;
     }
 
@@ -190,10 +219,11 @@ struct SphRay
 
         if (P.diskOn && trans > 0.01f)
         {
+            const CamFrame<R>& F = frame_of<R>(P);
             R sp, cp;
             sincos_fast(phi, sp, cp);
-            f3 pos = v3((float)((e1x * cp + e2x * sp) * r), (float)((e1y * cp + e2y * sp) * r),
-                        (float)((e1z * cp + e2z * sp) * r));
+            f3 pos = v3((float)((F.e1[0] * cp + e2x * sp) * r), (float)((F.e1[1] * cp + e2y * sp) * r),
+                        (float)((F.e1[2] * cp + e2z * sp) * r));
             disk_segment<STATS>(P, E, Lz, prevPos, pos, (float)((R)P.diskTime - tFlight),
                                 accum, trans, tally);
             prevPos = pos;
@@ -219,19 +249,20 @@ struct SphRay
         o.escDir = dir0;
         if (escaped && haveDir)
         {   // chord direction of the last step, rebuilt with accurate trig
+            const CamFrame<R>& F = frame_of<R>(P);
             R sp, cp;
             sincos(phid, &sp, &cp);
             R r = R(1) / ud;
             R drdphi = -dud / (ud * ud);
-            R mx = e1x * cp + e2x * sp, my = e1y * cp + e2y * sp, mz = e1z * cp + e2z * sp;
-            R qx = -e1x * sp + e2x * cp, qy = -e1y * sp + e2y * cp, qz = -e1z * sp + e2z * cp;
+            R mx = F.e1[0] * cp + e2x * sp, my = F.e1[1] * cp + e2y * sp, mz = F.e1[2] * cp + e2z * sp;
+            R qx = -F.e1[0] * sp + e2x * cp, qy = -F.e1[1] * sp + e2y * cp, qz = -F.e1[2] * sp + e2z * cp;
             o.escDir = normalize_x(v3((float)(mx * drdphi + qx * r), (float)(my * drdphi + qy * r),
                                       (float)(mz * drdphi + qz * r)));
         }
         if (STATS)
         {
             o.tally = tally;
-            double I1 = binet((R)P.M, (R)P.Q * (R)P.Q, u, du);
+            double I1 = (step > 0) ? binet((R)P.M, (R)P.Q * (R)P.Q, u, du) : I0;
             o.drift = (I0 > 0.0) ? (float)(fabs(I1 - I0) / I0) : 0.f;
         }
         else { o.drift = 0.f; o.tally.samples = 0; o.tally.hitR = 0.f; o.tally.hitG = 0.f; }
@@ -292,38 +323,17 @@ struct KerrRay
     double Q0;
 
     BH_DEV int init(const TraceParams& P, f3 dirf)
-    {   // reference src/trace.cuh:703-739, accurate library functions
-        const R M = (R)P.M, a = (R)P.a, Q = (R)P.Q;
-        vec3<R> o = widen<R>(tof3(P.camPos));
-        vec3<R> dir = widen<R>(dirf);
-        R r0 = sqrt_p(dot3(o, o));
-        R cth0 = min_p(max_p(o.y / r0, R(-1)), R(1));
-        R th0 = acos(cth0);
-        R ph0 = atan2(-o.z, o.x);
-        R s0r, c0, sp, cp;
-        sincos(th0, &s0r, &c0);
-        sincos(ph0, &sp, &cp);
-        R drc = dir.x * (s0r * cp) + dir.y * c0 + dir.z * (-s0r * sp);
-        R dtc = dir.x * (c0 * cp) + dir.y * (-s0r) + dir.z * (-c0 * sp);
-        R dpc = dir.x * (-sp) + dir.z * (-cp);
-        R s0 = max_p(s0r, R(1e-4f));
-        R s02 = s0 * s0;
-        R Sig0 = r0 * r0 + a * a * cth0 * cth0;
-        R Del0 = r0 * r0 - R(2) * M * r0 + a * a + Q * Q;
-        R m2r0 = R(2) * M * r0 - Q * Q;
-        R gtt = -(R(1) - m2r0 / Sig0);
-        if (gtt > R(-1e-5f)) gtt = R(-1e-5f);
-        R gtp = -a * m2r0 * s02 / Sig0;
-        R gpp = (r0 * r0 + a * a + m2r0 * a * a * s02 / Sig0) * s02;
-        R A = R(1) / sqrt_p(max_p(gpp - gtp * gtp / gtt, R(1e-8f)));
-        R ptUp = R(1) / sqrt_p(-gtt) - dpc * A * gtp / gtt;
-        R pfUp = dpc * A;
-        E = -(gtt * ptUp + gtp * pfUp);
-        Lz = gtp * ptUp + gpp * pfUp;
-
-        r = r0; th = th0; ph = ph0;
-        pr = drc * sqrt_p(Sig0 / max_p(Del0, R(1e-6f)));
-        pth = dtc * sqrt_p(Sig0);
+    {   // reference src/trace.cuh:703-739: the per-ray remainder of the tetrad map
+        const CamFrame<R>& F = frame_of<R>(P);
+        const vec3<R> dir = widen<R>(dirf);
+        R drc = xdot(F.er, dir), dtc = xdot(F.eth, dir), dpc = xdot(F.eph, dir);
+        R ptUp = xsub(F.rsq, xdiv(xmul(xmul(dpc, F.A), F.gtp), F.gtt));
+        R pfUp = xmul(dpc, F.A);
+        E = -xadd(xmul(F.gtt, ptUp), xmul(F.gtp, pfUp));
+        Lz = xadd(xmul(F.gtp, ptUp), xmul(F.gpp, pfUp));
+        r = F.r0; th = F.th0; ph = F.ph0;
+        pr = xmul(drc, F.sqSD);
+        pth = xmul(dtc, F.sqS);
         sincos_polar(th, s, c);
 
         tFlight = R(0);
@@ -337,7 +347,7 @@ struct KerrRay
         if (STATS)
         {
             tally.samples = 0; tally.hitR = 0.f; tally.hitG = 0.f;
-            Q0 = carterQ(th, pth, a, E, Lz);
+            Q0 = carterQ(th, pth, (R)P.a, E, Lz);
         }
         return RAY_LIVE;
     }
@@ -391,21 +401,21 @@ struct KerrRay
             capLen = max_p(R(1.2f), R(0.22f) * r);
         h = min_p(h, capLen * rcp_p(spd));
 
-        // classic RK4
+        // classic RK4; stage angles th + delta via angle addition from (s, c)
         const R hh = R(0.5f) * h;
         R Kx, sx, cx;
-        R yr = r + hh * d1.r, yth = th + hh * d1.th, ypr = pr + hh * d1.pr, ypth = pth + hh * d1.pth;
-        sincos_polar(yth, sx, cx);
+        R yr = r + hh * d1.r, ypr = pr + hh * d1.pr, ypth = pth + hh * d1.pth;
+        sincos_shift(th, s, c, hh * d1.th, sx, cx);
         KerrDeriv<R> d2 = kerr_rhs(M, a, Q2, E, Lz, yr, sx, cx, ypr, ypth, Kx);
         R sr = d1.r + R(2) * d2.r, sth = d1.th + R(2) * d2.th, sph = d1.ph + R(2) * d2.ph;
         R spr = d1.pr + R(2) * d2.pr, spth = d1.pth + R(2) * d2.pth;
-        yr = r + hh * d2.r; yth = th + hh * d2.th; ypr = pr + hh * d2.pr; ypth = pth + hh * d2.pth;
-        sincos_polar(yth, sx, cx);
+        yr = r + hh * d2.r; ypr = pr + hh * d2.pr; ypth = pth + hh * d2.pth;
+        sincos_shift(th, s, c, hh * d2.th, sx, cx);
         KerrDeriv<R> d3 = kerr_rhs(M, a, Q2, E, Lz, yr, sx, cx, ypr, ypth, Kx);
         sr += R(2) * d3.r; sth += R(2) * d3.th; sph += R(2) * d3.ph;
         spr += R(2) * d3.pr; spth += R(2) * d3.pth;
-        yr = r + h * d3.r; yth = th + h * d3.th; ypr = pr + h * d3.pr; ypth = pth + h * d3.pth;
-        sincos_polar(yth, sx, cx);
+        yr = r + h * d3.r; ypr = pr + h * d3.pr; ypth = pth + h * d3.pth;
+        sincos_shift(th, s, c, h * d3.th, sx, cx);
         KerrDeriv<R> d4 = kerr_rhs(M, a, Q2, E, Lz, yr, sx, cx, ypr, ypth, Kx);
         const R h6 = h * R(1.0 / 6.0);
         r += h6 * (sr + d4.r);

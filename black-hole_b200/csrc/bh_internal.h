@@ -24,5 +24,8 @@ cudaError_t bh_launch_trace(const TraceParams& P, int precision, bool stats, int
 cudaError_t bh_launch_post(uchar4* out, const float4* accum, float4* hblur, int W, int H,
                            const PostConsts& pc, cudaStream_t stream);
 
+// camera-frame constants of t.camPos / t.M / t.a / t.Q in FP32 and FP64 (bh_camera.cpp)
+void bh_fill_camera_frames(TraceParams& t);
+
 // FP32 FMA throughput probe (bh_peak.cu)
 double bh_measure_fp32_peak();

@@ -49,12 +49,14 @@ BH_DEV float clampf(float x, float lo, float hi) { return fminf(fmaxf(x, lo), hi
 BH_DEV double clampd(double x, double lo, double hi) { return fmin(fmax(x, lo), hi); }
 BH_DEV float smoothstep_f(float e0, float e1, float x)
 {
-    float t = clampf(__fdiv_rn(x - e0, e1 - e0), 0.f, 1.f);
+    float t = clampf(__fdividef(x - e0, e1 - e0), 0.f, 1.f);
     return t * t * (3.f - 2.f * t);
 }
 // fast reciprocal: one MUFU.RCP (relative error ~2^-23)
 BH_DEV float rcp_f(float x) { float r; asm("rcp.approx.ftz.f32 %0, %1;" : "=f"(r) : "f"(x)); return r; }
 BH_DEV float rsqrt_f(float x) { float r; asm("rsqrt.approx.ftz.f32 %0, %1;" : "=f"(r) : "f"(x)); return r; }
+// fast square root (MUFU based, relative error ~2^-22, sqrt(0) = 0)
+BH_DEV float sqrt_a(float x) { float r; asm("sqrt.approx.f32 %0, %1;" : "=f"(r) : "f"(x)); return r; }
 
 // ---- sin/cos ---------------------------------------------------------------------
 // Polynomial sincos for x in [0, pi] (the polar angle theta).  Reduce to

@@ -24,7 +24,7 @@ BH_DEV float omega_circ(float r, float M, float a, float Q)
 {
     float w2 = M * r - Q * Q;
     if (w2 <= 0.f) return 0.f;
-    float sw = sqrtf(w2);
+    float sw = sqrt_a(w2);
     return __fdividef(sw, r * r + a * sw);
 }
 
@@ -48,7 +48,7 @@ BH_DEV float thin_disk_flux(float r, float rIn)
 {
     if (!(r > rIn) || rIn <= 0.f) return 0.f;
     float x = __fdividef(rIn, r);
-    float nt = x * x * x * fmaxf(1.f - sqrtf(x), 0.f);
+    float nt = x * x * x * fmaxf(1.f - sqrt_a(x), 0.f);
     float dr = r - rIn * 1.15f;
     float sig = 0.20f * rIn;
     float peak = __expf(__fdividef(-0.5f * dr * dr, fmaxf(sig * sig, 1e-8f)));
@@ -145,18 +145,18 @@ BH_DEV void disk_segment(const TraceParams& P, float E, float Lz, f3 a, f3 b, fl
     if (a.y < -maxH && b.y < -maxH) return;
 
     f3 seg = b - a;
-    float segLen = sqrtf(dot3(seg, seg));
+    float segLen = sqrt_a(dot3(seg, seg));
     if (segLen < 1e-7f) return;
-    float rcA = sqrtf(a.x * a.x + a.z * a.z);
-    float rcB = sqrtf(b.x * b.x + b.z * b.z);
+    float rcA = sqrt_a(a.x * a.x + a.z * a.z);
+    float rcB = sqrt_a(b.x * b.x + b.z * b.z);
     if (fminf(rcA, rcB) - segLen > P.diskOuter) return;
     if (fmaxf(rcA, rcB) + segLen < P.diskInner) return;
 
     int nSub = 1 + (int)(segLen * 6.5f);
     if (nSub > 12) nSub = 12;
     const float fsub = (float)nSub;
-    const float ds = __fdiv_rn(segLen, fsub);
-    const float invSub = __frcp_rn(fsub);
+    const float invSub = rcp_f(fsub);
+    const float ds = segLen * invSub;
 
     const float rin = fmaxf(P.diskInner, 1e-4f);
     const float invOut = __frcp_rn(fmaxf(P.diskOuter, rin));
@@ -166,7 +166,7 @@ BH_DEV void disk_segment(const TraceParams& P, float E, float Lz, f3 a, f3 b, fl
     {
         float t = ((float)j + 0.5f) * invSub;
         f3 p = a + seg * t;
-        float rc = sqrtf(p.x * p.x + p.z * p.z);
+        float rc = sqrt_a(p.x * p.x + p.z * p.z);
         if (rc < rin || rc > P.diskOuter) continue;
 
         float H = (0.040f + 0.015f * (rc * invOut)) * rc;
@@ -220,7 +220,7 @@ BH_DEV void disk_segment(const TraceParams& P, float E, float Lz, f3 a, f3 b, fl
         }
         if (dens < 1e-5f && spotBoost < 1e-4f) continue;
 
-        float Temit = kTInner * sqrtf(sqrtf(clampf(Fr, 1e-6f, 1.f)));
+        float Temit = kTInner * sqrt_a(sqrt_a(clampf(Fr, 1e-6f, 1.f)));
         Temit = clampf(Temit * (1.f + 1.6f * spotHeat), 2000.f, 26000.f);
         f3 col = blackbody(clampf(Temit * g, 1200.f, 40000.f));
         float g3 = g * g * g;

@@ -2,15 +2,21 @@
 // bh_trace.cu -- persistent geodesic-tracing kernels for sm_100a.
 //
 // Work distribution.  A frame is a queue of rays in 8x4-pixel tiles (32
-// consecutive ray ids are one tile, so a warp that refills several lanes at
-// once gets neighbouring pixels with similar paths).  The grid is persistent:
-// blocks_per_SM x SM-count CTAs stay resident and every warp keeps 32 rays in
-// registers.  A ray that terminates leaves its lane idle; once at least
-// `refillMin` lanes of a warp are idle the warp, in one converged block,
-// shades and writes the finished rays and claims new ray ids for all idle
-// lanes with a single atomicAdd on the frame's ray counter.  Long photon-ring
-// rays therefore no longer hold 31 idle lanes hostage, which is the
-// divergence that dominates a one-thread-per-pixel launch.
+// consecutive ray ids form one tile, so rays claimed together are
+// neighbouring pixels with similar paths).  The grid is persistent: as many
+// 128-thread CTAs as fit stay resident on every SM, and each warp keeps 32
+// rays in registers.
+//
+//  * Refill.  When at least `refillMin` lanes of a warp are idle the warp
+//    hands them the next ray ids of its private range (one atomicAdd on the
+//    frame counter claims a whole 32-ray tile) and initialises them.  Per-ray
+//    initialisation is ~30 exact operations because the camera frame is
+//    precomputed (CamFrame), so refilling often is cheap.
+//  * Deferred shading.  A finished ray does not shade in place (that would run
+//    the ~1000-instruction sky model with one lane active): its result
+//    (32 bytes) is pushed onto a per-warp ring in shared memory and the lane
+//    is refilled at once.  Whenever 32 results are queued the whole warp
+//    shades them together, one per lane, fully converged.
 //
 // Families are separate kernels (template), so the step loop has no model
 // branch; R = float is the product path, R = double the GPU accuracy oracle.
@@ -20,57 +26,31 @@
 #include "bh_internal.h"
 #include "../../include/bh_launch.h"
 
-template <bool STATS>
-BH_DEV void write_ray(const TraceParams& P, unsigned rid, int px, int py, const RayResult& t)
-{
-    f3 hdr = t.accum;
-    if (!t.horizon)
-    {
-        f3 bg = sky_color(t.escDir, P.gCam);
-        hdr = v3(hdr.x + bg.x * t.trans, hdr.y + bg.y * t.trans, hdr.z + bg.z * t.trans);
-    }
-    if (!isfinite(hdr.x) || !isfinite(hdr.y) || !isfinite(hdr.z)) hdr = v3(0.f, 0.f, 0.f);
+namespace {
 
-    const size_t idx = P.dirs ? (size_t)rid : (size_t)py * P.W + px;
-    switch (P.outMode)
-    {
-    case BH_OUT_ACCUM:
-    {
-        float4* acc = reinterpret_cast<float4*>(P.out);
-        float4 pv = acc[idx];
-        f3 prev = v3(pv.x, pv.y, pv.z);
-        if (!isfinite(prev.x) || !isfinite(prev.y) || !isfinite(prev.z)) prev = hdr;
-        f3 c = accum_blend(prev, hdr, P.accumMode, P.sampleIndex);
-        acc[idx] = make_float4(c.x, c.y, c.z, 1.f);
-        break;
-    }
-    case BH_OUT_RGBA:
-    {
-        PostConsts pc{P.exposure, 0.f, 0, P.swapRB};
-        reinterpret_cast<uchar4*>(P.out)[idx] = finalize_pixel(hdr, v3(0.f, 0.f, 0.f), pc, px, py);
-        break;
-    }
-    case BH_OUT_HDR:
-        reinterpret_cast<float4*>(P.out)[idx] = make_float4(hdr.x, hdr.y, hdr.z, 1.f);
-        break;
-    default:
-    {
-        BHProbe o;
-        o.outcome = t.escaped ? 1 : 0;
-        o.cls = (t.trans < 0.5f) ? 1 : (t.horizon ? 0 : 2);
-        o.steps = t.steps;
-        o.diskSamples = t.tally.samples;
-        o.escDir[0] = t.escDir.x; o.escDir[1] = t.escDir.y; o.escDir[2] = t.escDir.z;
-        o.trans = t.trans;
-        o.accum[0] = t.accum.x; o.accum[1] = t.accum.y; o.accum[2] = t.accum.z;
-        o.maxHviol = t.maxHviol;
-        o.hdr[0] = hdr.x; o.hdr[1] = hdr.y; o.hdr[2] = hdr.z;
-        o.diskR = t.tally.hitR; o.diskG = t.tally.hitG; o.drift = t.drift;
-        reinterpret_cast<BHProbe*>(P.out)[idx] = o;
-        break;
-    }
-    }
-}
+constexpr int kWarps = BH_TRACE_BLOCK / 32;
+constexpr int kQueue = 64;            // ring entries per warp (>= 2 x 32)
+constexpr unsigned kChunk = 32;       // ray ids claimed per atomicAdd (one tile)
+constexpr unsigned kHorizon = 1u << 31, kEscaped = 1u << 30, kKeyMask = kEscaped - 1u;
+
+// Finished ray awaiting shading (32 bytes; the statistics half only in probe kernels).
+struct Slot
+{
+    unsigned key;        // pixel index or ray id | outcome flags
+    float esc[3];
+    float acc[3];
+    float trans;
+};
+struct SlotStats
+{
+    int steps, samples;
+    float maxHviol, drift, hitR, hitG;
+    int pad[2];
+};
+
+template <bool STATS> struct Queue;
+template <> struct Queue<false> { Slot s[kWarps][kQueue]; };
+template <> struct Queue<true> { Slot s[kWarps][kQueue]; SlotStats t[kWarps][kQueue]; };
 
 // ray id -> pixel (8x4 tiles, row-major tile order); false when outside the frame
 BH_DEV bool ray_pixel(const TraceParams& P, unsigned rid, int& px, int& py)
@@ -93,70 +73,176 @@ BH_DEV f3 ray_direction(const TraceParams& P, unsigned rid, int px, int py)
     return camera_ray(P, fx, fy);
 }
 
+// Shade one queued result (sky behind the ray) and write it in the output mode.
+template <bool STATS>
+BH_DEV void shade_slot(const TraceParams& P, const Slot& q, const SlotStats* qs)
+{
+    const bool horizon = (q.key & kHorizon) != 0u, escaped = (q.key & kEscaped) != 0u;
+    const unsigned key = q.key & kKeyMask;
+    f3 hdr = v3(q.acc[0], q.acc[1], q.acc[2]);
+    if (!horizon)
+    {
+        f3 bg = sky_color(v3(q.esc[0], q.esc[1], q.esc[2]), P.gCam);
+        hdr = v3(hdr.x + bg.x * q.trans, hdr.y + bg.y * q.trans, hdr.z + bg.z * q.trans);
+    }
+    if (!isfinite(hdr.x) || !isfinite(hdr.y) || !isfinite(hdr.z)) hdr = v3(0.f, 0.f, 0.f);
+
+    switch (P.outMode)
+    {
+    case BH_OUT_ACCUM:
+    {
+        float4* acc = reinterpret_cast<float4*>(P.out);
+        float4 pv = acc[key];
+        f3 prev = v3(pv.x, pv.y, pv.z);
+        if (!isfinite(prev.x) || !isfinite(prev.y) || !isfinite(prev.z)) prev = hdr;
+        f3 c = accum_blend(prev, hdr, P.accumMode, P.sampleIndex);
+        acc[key] = make_float4(c.x, c.y, c.z, 1.f);
+        break;
+    }
+    case BH_OUT_RGBA:
+    {
+        const int py = (int)(key / (unsigned)P.W), px = (int)(key - (unsigned)py * (unsigned)P.W);
+        PostConsts pc{P.exposure, 0.f, 0, P.swapRB};
+        reinterpret_cast<uchar4*>(P.out)[key] = finalize_pixel(hdr, v3(0.f, 0.f, 0.f), pc, px, py);
+        break;
+    }
+    case BH_OUT_HDR:
+        reinterpret_cast<float4*>(P.out)[key] = make_float4(hdr.x, hdr.y, hdr.z, 1.f);
+        break;
+    default:
+    {
+        BHProbe o;
+        o.outcome = escaped ? 1 : 0;
+        o.cls = (q.trans < 0.5f) ? 1 : (horizon ? 0 : 2);
+        o.steps = STATS ? qs->steps : 0;
+        o.diskSamples = STATS ? qs->samples : 0;
+        o.escDir[0] = q.esc[0]; o.escDir[1] = q.esc[1]; o.escDir[2] = q.esc[2];
+        o.trans = q.trans;
+        o.accum[0] = q.acc[0]; o.accum[1] = q.acc[1]; o.accum[2] = q.acc[2];
+        o.maxHviol = STATS ? qs->maxHviol : 0.f;
+        o.hdr[0] = hdr.x; o.hdr[1] = hdr.y; o.hdr[2] = hdr.z;
+        o.diskR = STATS ? qs->hitR : 0.f;
+        o.diskG = STATS ? qs->hitG : 0.f;
+        o.drift = STATS ? qs->drift : 0.f;
+        reinterpret_cast<BHProbe*>(P.out)[key] = o;
+        break;
+    }
+    }
+}
+
 template <class Ray, bool STATS>
 __global__ void __launch_bounds__(BH_TRACE_BLOCK)
 trace_kernel(const __grid_constant__ TraceParams P)
 {
-    const unsigned lane = threadIdx.x & 31u;
-    const unsigned FULL = 0xffffffffu;
+    __shared__ Queue<STATS> Q;
+    const unsigned lane = threadIdx.x & 31u, warp = threadIdx.x >> 5;
+    const unsigned FULL = 0xffffffffu, below = (1u << lane) - 1u;
+    Slot* ring = Q.s[warp];
+
     Ray ray;
-    unsigned rid = 0;
-    int px = 0, py = 0;
-    bool live = false, pending = false, exhausted = false;
+    unsigned rid = 0, key = 0;
+    bool live = false;
+    unsigned next = 0, end = 0;          // warp-private ray-id range (warp-uniform)
+    bool drained = false;                // frame counter exhausted (warp-uniform)
+    unsigned qHead = 0, qTail = 0;       // ring cursors (warp-uniform)
 
     while (true)
     {
+        bool fin = false;
         const unsigned liveMask = __ballot_sync(FULL, live);
-        const int nFree = 32 - __popc(liveMask);
-        if (liveMask == 0u || (!exhausted && nFree >= P.refillMin))
+        const unsigned nFree = 32u - (unsigned)__popc(liveMask);
+        const bool haveWork = !drained || next < end;
+        if (haveWork && (liveMask == 0u || nFree >= (unsigned)P.refillMin))
         {
-            if (pending)
+            // hand ids to the idle lanes, claiming a new tile if the range runs short
+            unsigned avail = end - next, base = 0;
+            bool claimed = false;
+            if (avail < nFree && !drained)
             {
-                RayResult t;
-                ray.result(P, ray_direction(P, rid, px, py), t);
-                write_ray<STATS>(P, rid, px, py, t);
-                pending = false;
+                if (lane == 0) base = atomicAdd(P.counter, kChunk);
+                base = __shfl_sync(FULL, base, 0);
+                claimed = true;
+                if (base + kChunk >= P.nRays) drained = true;
             }
-            if (exhausted)
-            {
-                if (liveMask == 0u) break;
-                continue;
-            }
-            unsigned base = 0;
-            if (lane == 0) base = atomicAdd(P.counter, (unsigned)nFree);
-            base = __shfl_sync(FULL, base, 0);
             if (!live)
             {
-                const unsigned rank = __popc(~liveMask & ((1u << lane) - 1u));
-                const unsigned id = base + rank;
-                if (id < P.nRays)
+                const unsigned rank = (unsigned)__popc(~liveMask & below);
+                unsigned id = (rank < avail) ? next + rank : base + (rank - avail);
+                bool valid = (rank < avail) || (claimed && base < P.nRays);
+                if (valid && id < P.nRays)
                 {
-                    rid = id;
-                    bool inFrame = true;
-                    if (!P.dirs) inFrame = ray_pixel(P, rid, px, py);
+                    int px = 0, py = 0;
+                    bool inFrame = P.dirs ? true : ray_pixel(P, id, px, py);
                     if (inFrame)
                     {
-                        int st = ray.init(P, ray_direction(P, rid, px, py));
+                        rid = id;
+                        key = P.dirs ? id : (unsigned)py * (unsigned)P.W + (unsigned)px;
+                        int st = ray.init(P, ray_direction(P, id, px, py));
                         live = (st == RAY_LIVE);
-                        pending = (st == RAY_DONE);
+                        fin = (st == RAY_DONE);
                     }
                 }
             }
-            if (base + (unsigned)nFree >= P.nRays) exhausted = true;
-            continue;
+            if (avail >= nFree) next += nFree;
+            else if (claimed && base < P.nRays)
+            {
+                end = min(base + kChunk, P.nRays);
+                next = min(base + (nFree - avail), end);
+            }
+            else next = end;
         }
-        if (live && ray.advance(P))
+        else if (liveMask == 0u)
         {
-            live = false;
-            pending = true;
+            break;   // no rays left for this warp
+        }
+
+        if (live && ray.advance(P)) { live = false; fin = true; }
+
+        const unsigned finMask = __ballot_sync(FULL, fin);
+        if (finMask)
+        {
+            if (fin)
+            {
+                const unsigned slot = (qTail + (unsigned)__popc(finMask & below)) & (kQueue - 1);
+                int px = 0, py = 0;
+                if (!P.dirs) { py = (int)(key / (unsigned)P.W); px = (int)(key - (unsigned)py * (unsigned)P.W); }
+                RayResult t;
+                ray.result(P, ray_direction(P, rid, px, py), t);
+                Slot& q = ring[slot];
+                q.key = key | (t.horizon ? kHorizon : 0u) | (t.escaped ? kEscaped : 0u);
+                q.esc[0] = t.escDir.x; q.esc[1] = t.escDir.y; q.esc[2] = t.escDir.z;
+                q.acc[0] = t.accum.x; q.acc[1] = t.accum.y; q.acc[2] = t.accum.z;
+                q.trans = t.trans;
+                if constexpr (STATS)
+                {
+                    SlotStats& s = Q.t[warp][slot];
+                    s.steps = t.steps; s.samples = t.tally.samples;
+                    s.maxHviol = t.maxHviol; s.drift = t.drift; s.hitR = t.tally.hitR; s.hitG = t.tally.hitG;
+                }
+            }
+            qTail += (unsigned)__popc(finMask);
+            __syncwarp();
+            if (qTail - qHead >= 32u)
+            {
+                const unsigned slot = (qHead + lane) & (kQueue - 1);
+                const SlotStats* qs = nullptr;
+                if constexpr (STATS) qs = &Q.t[warp][slot];
+                shade_slot<STATS>(P, ring[slot], qs);
+                qHead += 32u;
+                __syncwarp();
+            }
         }
     }
+    // shade what is left in the ring
+    __syncwarp();
+    if (lane < qTail - qHead)
+    {
+        const unsigned slot = (qHead + lane) & (kQueue - 1);
+        const SlotStats* qs = nullptr;
+        if constexpr (STATS) qs = &Q.t[warp][slot];
+        shade_slot<STATS>(P, ring[slot], qs);
+    }
 }
-
-// ---------------------------------------------------------------------------
-// host side
-// ---------------------------------------------------------------------------
-namespace {
 
 template <class Ray, bool STATS>
 cudaError_t launch_one(const TraceParams& P, int blocksPerSm, cudaStream_t stream)

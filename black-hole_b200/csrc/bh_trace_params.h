@@ -2,9 +2,9 @@
 // ---------------------------------------------------------------------------
 // bh_trace_params.h -- per-launch constants of the tracing kernels (host and
 // device).  Built on the host from a sanitised RenderParams once per frame, so
-// frame-invariant quantities (camera energy factor, capture and escape radii,
-// jitter) are computed once instead of once per ray, and passed to the kernel
-// as a __grid_constant__ parameter (constant-bank operands, no loads).
+// frame-invariant quantities (camera energy factor, jitter, and the whole
+// static-observer tetrad at the camera) are computed once instead of once per
+// ray, and passed to the kernel as a __grid_constant__ parameter.
 // ---------------------------------------------------------------------------
 #include <cuda_runtime_api.h>
 #include <vector_types.h>
@@ -16,6 +16,28 @@ enum BhOutMode
     BH_OUT_RGBA = 1,    // finalise straight to uchar4 (no bloom): launchRenderKernel
     BH_OUT_HDR = 2,     // write the HDR sample as float4
     BH_OUT_PROBE = 3,   // write a BHProbe record per ray
+};
+
+// Camera-frame quantities shared by every ray of a view, in the integration
+// precision T.  They are the per-ray prologue of the reference integrators
+// (src/trace.cuh:213-247, 490-521, 703-739 of Sqhh99/Black-hole) with
+// everything that does not depend on the ray direction hoisted out; the host
+// evaluates them with the same float (or double) libm arithmetic as the
+// reference, so the per-ray remainder reproduces its initial data exactly.
+template <class T>
+struct CamFrame
+{
+    // rotating family
+    T r0, th0, ph0;
+    T er[3], eth[3], eph[3];     // orthonormal (r, theta, phi) basis at the camera
+    T gtt, gtp, gpp, A, rsq;     // metric at the camera, A = (gpp - gtp^2/gtt)^-1/2, rsq = (-gtt)^-1/2
+    T sqSD, sqS;                 // sqrt(Sigma / max(Delta, 1e-6)), sqrt(Sigma)
+    // spherical family
+    T e1[3];                     // radial unit vector camPos / r0
+    T ephS[3];                   // azimuthal unit vector of the photon-constant tetrad
+    T gttS, gtpS, gppS, AS, rsqS;
+    T f0, sf0, u0;               // max(f(r0), 1e-6), sqrt(f0), 1/r0
+    int camAtOrigin;             // r0 < 1e-4: E = 1, Lz = 0
 };
 
 struct TraceParams
@@ -54,4 +76,7 @@ struct TraceParams
     // work distribution
     unsigned* counter;            // ray counter, zeroed before the launch
     int refillMin;                // refill a warp when at least this many lanes are free
+
+    CamFrame<float> cf;           // FP32 integration
+    CamFrame<double> cd;          // FP64 integration
 };
