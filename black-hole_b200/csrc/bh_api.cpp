@@ -11,7 +11,7 @@
 #include <cmath>
 #include <mutex>
 #include <cuda_runtime.h>
-#include "../../include/bh_launch.h"
+#include "bh_launch.h"
 #include "bh_internal.h"
 
 namespace {

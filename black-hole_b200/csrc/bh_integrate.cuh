@@ -2,7 +2,7 @@
 // ---------------------------------------------------------------------------
 // bh_integrate.cuh -- the two geodesic integrators as resumable ray objects.
 //
-// Each integrator is split into init() / advance() / result() so that a warp
+// Each integrator is split into init() / advance() / pack() so that a warp
 // can hold 32 independent rays in registers and refill any lane whose ray
 // ended (bh_trace.cu).  The arithmetic per step is the reference's method
 // (Sqhh99/Black-hole):
@@ -32,16 +32,29 @@
 // ---------------------------------------------------------------------------
 #include "bh_shade.cuh"
 
-struct RayResult
+enum { RAY_SKIP = 0, RAY_LIVE = 1, RAY_DONE = 2 };
+
+// A finished ray as it waits for shading: outcome flags, the radiance gathered
+// from the disk, and the six state values from which the escape direction is
+// rebuilt at shading time (so the finishing lane only stores, and the
+// trigonometry runs later with the whole warp converged).
+constexpr unsigned kRayHorizon = 1u << 31, kRayEscaped = 1u << 30, kRayUseState = 1u << 29;
+constexpr unsigned kRayKeyMask = kRayUseState - 1u;
+
+template <class R>
+struct PackedRay
 {
-    bool horizon, escaped;
-    f3 escDir, accum;
-    float trans, maxHviol, drift;
-    int steps;
-    DiskTally tally;
+    unsigned key;         // pixel index or ray id | kRay* flags
+    float acc[3];
+    float trans;
+    R f[6];               // family-specific escape state
 };
 
-enum { RAY_SKIP = 0, RAY_LIVE = 1, RAY_DONE = 2 };
+struct PackedStats
+{
+    int steps, samples;
+    float maxHviol, drift, hitR, hitG;
+};
 
 // ---- exact single operations in either precision --------------------------------
 BH_DEV float xmul(float a, float b) { return __fmul_rn(a, b); }
@@ -114,6 +127,7 @@ BH_DEV void sincos_shift(double th, double, double, double delta, double& so, do
 template <class R, bool STATS>
 struct SphRay
 {
+    using Real = R;
     R u, du, phi, tFlight, invB;
     R e2x, e2y, e2z;                  // in-plane unit vector normal to e1 (e1 is the camera's)
     R ud, dud, phid;                  // state of the last chord direction (deferred)
@@ -241,31 +255,36 @@ struct SphRay
         else escaped = true;
     }
 
-    BH_DEV void result(const TraceParams& P, f3 dir0, RayResult& o) const
+    BH_DEV void pack(const TraceParams& P, unsigned key, PackedRay<R>& q, PackedStats* st) const
     {
-        o.horizon = horizon; o.escaped = escaped;
-        o.accum = accum; o.trans = trans; o.steps = step;
-        o.maxHviol = 0.f;
-        o.escDir = dir0;
-        if (escaped && haveDir)
-        {   // chord direction of the last step, rebuilt with accurate trig
-            const CamFrame<R>& F = frame_of<R>(P);
-            R sp, cp;
-            sincos(phid, &sp, &cp);
-            R r = R(1) / ud;
-            R drdphi = -dud / (ud * ud);
-            R mx = F.e1[0] * cp + e2x * sp, my = F.e1[1] * cp + e2y * sp, mz = F.e1[2] * cp + e2z * sp;
-            R qx = -F.e1[0] * sp + e2x * cp, qy = -F.e1[1] * sp + e2y * cp, qz = -F.e1[2] * sp + e2z * cp;
-            o.escDir = normalize_x(v3((float)(mx * drdphi + qx * r), (float)(my * drdphi + qy * r),
-                                      (float)(mz * drdphi + qz * r)));
-        }
+        const bool useState = escaped && haveDir;
+        q.key = key | (horizon ? kRayHorizon : 0u) | (escaped ? kRayEscaped : 0u) | (useState ? kRayUseState : 0u);
+        q.acc[0] = accum.x; q.acc[1] = accum.y; q.acc[2] = accum.z;
+        q.trans = trans;
+        q.f[0] = ud; q.f[1] = dud; q.f[2] = phid; q.f[3] = e2x; q.f[4] = e2y; q.f[5] = e2z;
         if (STATS)
         {
-            o.tally = tally;
+            st->steps = step; st->samples = tally.samples; st->maxHviol = 0.f;
+            st->hitR = tally.hitR; st->hitG = tally.hitG;
             double I1 = (step > 0) ? binet((R)P.M, (R)P.Q * (R)P.Q, u, du) : I0;
-            o.drift = (I0 > 0.0) ? (float)(fabs(I1 - I0) / I0) : 0.f;
+            st->drift = (I0 > 0.0) ? (float)(fabs(I1 - I0) / I0) : 0.f;
         }
-        else { o.drift = 0.f; o.tally.samples = 0; o.tally.hitR = 0.f; o.tally.hitG = 0.f; }
+    }
+
+    // Escape direction: the chord direction of the last step (reference
+    // src/trace.cuh:581-587), rebuilt with accurate trigonometry.
+    BH_DEV static f3 escape_dir(const TraceParams& P, const PackedRay<R>& q)
+    {
+        const CamFrame<R>& F = frame_of<R>(P);
+        const R ud_ = q.f[0], dud_ = q.f[1], phid_ = q.f[2], ex = q.f[3], ey = q.f[4], ez = q.f[5];
+        R sp, cp;
+        sincos(phid_, &sp, &cp);
+        R r = R(1) / ud_;
+        R drdphi = -dud_ / (ud_ * ud_);
+        R mx = F.e1[0] * cp + ex * sp, my = F.e1[1] * cp + ey * sp, mz = F.e1[2] * cp + ez * sp;
+        R qx = -F.e1[0] * sp + ex * cp, qy = -F.e1[1] * sp + ey * cp, qz = -F.e1[2] * sp + ez * cp;
+        return normalize_x(v3((float)(mx * drdphi + qx * r), (float)(my * drdphi + qy * r),
+                              (float)(mz * drdphi + qz * r)));
     }
 };
 
@@ -311,6 +330,7 @@ BH_DEV KerrDeriv<R> kerr_rhs(R M, R a, R Q2, R E, R Lz, R r, R s, R c, R pr, R p
 template <class R, bool STATS>
 struct KerrRay
 {
+    using Real = R;
     R r, th, ph, pr, pth;   // Boyer-Lindquist state
     R s, c;                 // sin/cos of th, carried between steps
     R E, Lz, tFlight;
@@ -459,31 +479,35 @@ struct KerrRay
         else { escaped = true; useDeriv = step > 0; }
     }
 
-    BH_DEV void result(const TraceParams& P, f3 dir0, RayResult& o) const
+    BH_DEV void pack(const TraceParams& P, unsigned key, PackedRay<R>& q, PackedStats* st) const
     {
-        o.horizon = horizon; o.escaped = escaped;
-        o.accum = accum; o.trans = trans; o.steps = step;
-        o.maxHviol = STATS ? maxHviol : 0.f;
-        o.escDir = dir0;
-        if (escaped && useDeriv)
-        {   // kerrBasis(th, ph) applied to the coordinate derivative, accurate trig
-            R sth, cth, sph, cph;
-            sincos(th, &sth, &cth);
-            sincos(ph, &sph, &cph);
-            R vr = dr_, vt = r * dth_, vp = r * sth * dph_;
-            f3 d = v3((float)(sth * cph * vr + cth * cph * vt - sph * vp),
-                      (float)(cth * vr - sth * vt),
-                      (float)(-sth * sph * vr - cth * sph * vt - cph * vp));
-            o.escDir = normalize_x(d);
-        }
+        const bool useState = escaped && useDeriv;
+        q.key = key | (horizon ? kRayHorizon : 0u) | (escaped ? kRayEscaped : 0u) | (useState ? kRayUseState : 0u);
+        q.acc[0] = accum.x; q.acc[1] = accum.y; q.acc[2] = accum.z;
+        q.trans = trans;
+        q.f[0] = r; q.f[1] = th; q.f[2] = ph; q.f[3] = dr_; q.f[4] = dth_; q.f[5] = dph_;
         if (STATS)
         {
-            o.tally = tally;
+            st->steps = step; st->samples = tally.samples; st->maxHviol = maxHviol;
+            st->hitR = tally.hitR; st->hitG = tally.hitG;
             const R a = (R)P.a;
             double q1 = carterQ(th, pth, a, E, Lz);
             double scale = fabs(Q0) + (double)Lz * Lz + (double)a * a * (double)E * E;
-            o.drift = scale > 0.0 ? (float)(fabs(q1 - Q0) / scale) : 0.f;
+            st->drift = scale > 0.0 ? (float)(fabs(q1 - Q0) / scale) : 0.f;
         }
-        else { o.drift = 0.f; o.tally.samples = 0; o.tally.hitR = 0.f; o.tally.hitG = 0.f; }
+    }
+
+    // Escape direction: kerrBasis(th, ph) applied to the coordinate derivative
+    // (reference src/trace.cuh:775-779, 880-884), accurate trigonometry.
+    BH_DEV static f3 escape_dir(const TraceParams&, const PackedRay<R>& q)
+    {
+        const R r_ = q.f[0], th_ = q.f[1], ph_ = q.f[2];
+        R sth, cth, sph, cph;
+        sincos(th_, &sth, &cth);
+        sincos(ph_, &sph, &cph);
+        R vr = q.f[3], vt = r_ * q.f[4], vp = r_ * sth * q.f[5];
+        return normalize_x(v3((float)(sth * cph * vr + cth * cph * vt - sph * vp),
+                              (float)(cth * vr - sth * vt),
+                              (float)(-sth * sph * vr - cth * sph * vt - cph * vp)));
     }
 };

@@ -14,7 +14,7 @@
 // results are bit-identical to a host build of the reference.
 // ---------------------------------------------------------------------------
 #include <cmath>
-#include "../../include/bh_launch.h"
+#include "bh_launch.h"
 
 namespace {
 

@@ -13,10 +13,11 @@
 //    initialisation is ~30 exact operations because the camera frame is
 //    precomputed (CamFrame), so refilling often is cheap.
 //  * Deferred shading.  A finished ray does not shade in place (that would run
-//    the ~1000-instruction sky model with one lane active): its result
-//    (32 bytes) is pushed onto a per-warp ring in shared memory and the lane
-//    is refilled at once.  Whenever 32 results are queued the whole warp
-//    shades them together, one per lane, fully converged.
+//    the ~1000-instruction sky model with one lane active): its packed state
+//    (key, disk radiance, transmittance and six escape-state values) is stored
+//    on a per-warp ring in shared memory and the lane is free at once.
+//    Whenever 32 rays are queued the whole warp rebuilds their escape
+//    directions and shades them together, one per lane, fully converged.
 //
 // Families are separate kernels (template), so the step loop has no model
 // branch; R = float is the product path, R = double the GPU accuracy oracle.
@@ -24,33 +25,17 @@
 #include "bh_integrate.cuh"
 #include "bh_post.cuh"
 #include "bh_internal.h"
-#include "../../include/bh_launch.h"
+#include "bh_launch.h"
 
 namespace {
 
 constexpr int kWarps = BH_TRACE_BLOCK / 32;
 constexpr int kQueue = 64;            // ring entries per warp (>= 2 x 32)
 constexpr unsigned kChunk = 32;       // ray ids claimed per atomicAdd (one tile)
-constexpr unsigned kHorizon = 1u << 31, kEscaped = 1u << 30, kKeyMask = kEscaped - 1u;
 
-// Finished ray awaiting shading (32 bytes; the statistics half only in probe kernels).
-struct Slot
-{
-    unsigned key;        // pixel index or ray id | outcome flags
-    float esc[3];
-    float acc[3];
-    float trans;
-};
-struct SlotStats
-{
-    int steps, samples;
-    float maxHviol, drift, hitR, hitG;
-    int pad[2];
-};
-
-template <bool STATS> struct Queue;
-template <> struct Queue<false> { Slot s[kWarps][kQueue]; };
-template <> struct Queue<true> { Slot s[kWarps][kQueue]; SlotStats t[kWarps][kQueue]; };
+template <class R, bool STATS> struct Queue;
+template <class R> struct Queue<R, false> { PackedRay<R> s[kWarps][kQueue]; };
+template <class R> struct Queue<R, true> { PackedRay<R> s[kWarps][kQueue]; PackedStats t[kWarps][kQueue]; };
 
 // ray id -> pixel (8x4 tiles, row-major tile order); false when outside the frame
 BH_DEV bool ray_pixel(const TraceParams& P, unsigned rid, int& px, int& py)
@@ -73,16 +58,21 @@ BH_DEV f3 ray_direction(const TraceParams& P, unsigned rid, int px, int py)
     return camera_ray(P, fx, fy);
 }
 
-// Shade one queued result (sky behind the ray) and write it in the output mode.
-template <bool STATS>
-BH_DEV void shade_slot(const TraceParams& P, const Slot& q, const SlotStats* qs)
+// Shade one queued ray (sky behind it) and write it in the output mode.
+template <class Ray, bool STATS>
+BH_DEV void shade_slot(const TraceParams& P, const PackedRay<typename Ray::Real>& q, const PackedStats* qs)
 {
-    const bool horizon = (q.key & kHorizon) != 0u, escaped = (q.key & kEscaped) != 0u;
-    const unsigned key = q.key & kKeyMask;
+    const bool horizon = (q.key & kRayHorizon) != 0u, escaped = (q.key & kRayEscaped) != 0u;
+    const unsigned key = q.key & kRayKeyMask;
+    int px = 0, py = 0;
+    if (!P.dirs) { py = (int)(key / (unsigned)P.W); px = (int)(key - (unsigned)py * (unsigned)P.W); }
+    f3 esc = v3(0.f, 0.f, 0.f);
+    if (escaped)
+        esc = (q.key & kRayUseState) ? Ray::escape_dir(P, q) : ray_direction(P, key, px, py);
     f3 hdr = v3(q.acc[0], q.acc[1], q.acc[2]);
     if (!horizon)
     {
-        f3 bg = sky_color(v3(q.esc[0], q.esc[1], q.esc[2]), P.gCam);
+        f3 bg = sky_color(esc, P.gCam);
         hdr = v3(hdr.x + bg.x * q.trans, hdr.y + bg.y * q.trans, hdr.z + bg.z * q.trans);
     }
     if (!isfinite(hdr.x) || !isfinite(hdr.y) || !isfinite(hdr.z)) hdr = v3(0.f, 0.f, 0.f);
@@ -101,7 +91,6 @@ BH_DEV void shade_slot(const TraceParams& P, const Slot& q, const SlotStats* qs)
     }
     case BH_OUT_RGBA:
     {
-        const int py = (int)(key / (unsigned)P.W), px = (int)(key - (unsigned)py * (unsigned)P.W);
         PostConsts pc{P.exposure, 0.f, 0, P.swapRB};
         reinterpret_cast<uchar4*>(P.out)[key] = finalize_pixel(hdr, v3(0.f, 0.f, 0.f), pc, px, py);
         break;
@@ -116,7 +105,8 @@ BH_DEV void shade_slot(const TraceParams& P, const Slot& q, const SlotStats* qs)
         o.cls = (q.trans < 0.5f) ? 1 : (horizon ? 0 : 2);
         o.steps = STATS ? qs->steps : 0;
         o.diskSamples = STATS ? qs->samples : 0;
-        o.escDir[0] = q.esc[0]; o.escDir[1] = q.esc[1]; o.escDir[2] = q.esc[2];
+        if (!escaped) esc = ray_direction(P, key, px, py);   // reference keeps the initial direction
+        o.escDir[0] = esc.x; o.escDir[1] = esc.y; o.escDir[2] = esc.z;
         o.trans = q.trans;
         o.accum[0] = q.acc[0]; o.accum[1] = q.acc[1]; o.accum[2] = q.acc[2];
         o.maxHviol = STATS ? qs->maxHviol : 0.f;
@@ -134,10 +124,11 @@ template <class Ray, bool STATS>
 __global__ void __launch_bounds__(BH_TRACE_BLOCK)
 trace_kernel(const __grid_constant__ TraceParams P)
 {
-    __shared__ Queue<STATS> Q;
+    using R = typename Ray::Real;
+    __shared__ Queue<R, STATS> Q;
     const unsigned lane = threadIdx.x & 31u, warp = threadIdx.x >> 5;
     const unsigned FULL = 0xffffffffu, below = (1u << lane) - 1u;
-    Slot* ring = Q.s[warp];
+    PackedRay<R>* ring = Q.s[warp];
 
     Ray ray;
     unsigned rid = 0, key = 0;
@@ -204,30 +195,18 @@ trace_kernel(const __grid_constant__ TraceParams P)
             if (fin)
             {
                 const unsigned slot = (qTail + (unsigned)__popc(finMask & below)) & (kQueue - 1);
-                int px = 0, py = 0;
-                if (!P.dirs) { py = (int)(key / (unsigned)P.W); px = (int)(key - (unsigned)py * (unsigned)P.W); }
-                RayResult t;
-                ray.result(P, ray_direction(P, rid, px, py), t);
-                Slot& q = ring[slot];
-                q.key = key | (t.horizon ? kHorizon : 0u) | (t.escaped ? kEscaped : 0u);
-                q.esc[0] = t.escDir.x; q.esc[1] = t.escDir.y; q.esc[2] = t.escDir.z;
-                q.acc[0] = t.accum.x; q.acc[1] = t.accum.y; q.acc[2] = t.accum.z;
-                q.trans = t.trans;
-                if constexpr (STATS)
-                {
-                    SlotStats& s = Q.t[warp][slot];
-                    s.steps = t.steps; s.samples = t.tally.samples;
-                    s.maxHviol = t.maxHviol; s.drift = t.drift; s.hitR = t.tally.hitR; s.hitG = t.tally.hitG;
-                }
+                PackedStats* st = nullptr;
+                if constexpr (STATS) st = &Q.t[warp][slot];
+                ray.pack(P, key, ring[slot], st);
             }
             qTail += (unsigned)__popc(finMask);
             __syncwarp();
             if (qTail - qHead >= 32u)
             {
                 const unsigned slot = (qHead + lane) & (kQueue - 1);
-                const SlotStats* qs = nullptr;
+                const PackedStats* qs = nullptr;
                 if constexpr (STATS) qs = &Q.t[warp][slot];
-                shade_slot<STATS>(P, ring[slot], qs);
+                shade_slot<Ray, STATS>(P, ring[slot], qs);
                 qHead += 32u;
                 __syncwarp();
             }
@@ -238,9 +217,9 @@ trace_kernel(const __grid_constant__ TraceParams P)
     if (lane < qTail - qHead)
     {
         const unsigned slot = (qHead + lane) & (kQueue - 1);
-        const SlotStats* qs = nullptr;
+        const PackedStats* qs = nullptr;
         if constexpr (STATS) qs = &Q.t[warp][slot];
-        shade_slot<STATS>(P, ring[slot], qs);
+        shade_slot<Ray, STATS>(P, ring[slot], qs);
     }
 }
 
