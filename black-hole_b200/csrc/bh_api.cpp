@@ -43,7 +43,7 @@ cudaError_t deviceScratch(unsigned** out)
 // ---- tuning (set by bhSetTuning / the autotuner) ------------------------------
 struct Tuning
 {
-    int refillMin = 8;      // refill a warp when this many lanes are idle
+    int refillMin = 32;     // refill a warp when this many lanes are idle
     int blocksPerSm = 0;    // 0: as many as occupancy allows
 };
 Tuning gTune[2];            // [0] spherical family, [1] rotating family

@@ -30,7 +30,7 @@ template <class T> inline T fmaxT(T a, T b) { return std::fmax(a, b); }
 template <class T> inline T fminT(T a, T b) { return std::fmin(a, b); }
 
 template <class T>
-void fill(CamFrame<T>& f, float3 pos, float Mf, float af, float Qf)
+void fill(CamFrame<T>& f, const TraceParams& t, float3 pos, float Mf, float af, float Qf)
 {
     const T M = (T)Mf, a = (T)af, Q = (T)Qf;
     const T ox = (T)pos.x, oy = (T)pos.y, oz = (T)pos.z;
@@ -89,12 +89,32 @@ void fill(CamFrame<T>& f, float3 pos, float Mf, float af, float Qf)
     f.f0 = fmaxT(T(1) - T(2) * M / r0 + Q * Q / (r0 * r0), T(1e-6f));
     f.sf0 = sqrtT(f.f0);
     f.u0 = T(1) / r0;
+
+    // ---- step-loop constants: trace.cuh:477-482, 537, 548-550, 607, 696-701, 761-808, 874
+    const T rCap = (T)t.rCap, dPhi = (T)t.dPhi;
+    f.M = M; f.a = a; f.Q2 = Q * Q; f.a2 = a * a;
+    f.capR = rCap * T(1.002f) + T(1e-3f);
+    f.rFloor = fmaxT((T)t.rPlus, rCap);
+    f.rFloor105 = f.rFloor * T(1.05f);
+    f.escR = T(120) * M;
+    f.sixM = T(6) * M;
+    f.k8dPhi = T(8.0f) * dPhi;
+    f.i22dPhi = T(1) / (T(2.2f) * dPhi);
+    f.rPh15 = T(1.5f) * (T)t.rPhoton;
+    f.outer13 = (T)t.diskOuter * T(1.3f);
+    f.dPhi = dPhi;
+    f.hMin = dPhi * T(0.03f);
+    f.uHor = T(1) / fmaxT(rCap, T(1e-6f));
+    f.uEscape = T(1) / (T(120) * M);
+    f.invNineM = T(1) / (T(9) * M);
+    f.uPh = T(1) / fmaxT(T(1.5f) * (T)t.rPhoton, T(3) * M);
+    f.diskTime = (T)t.diskTime;
 }
 
 }  // namespace
 
 void bh_fill_camera_frames(TraceParams& t)
 {
-    fill(t.cf, t.camPos, t.M, t.a, t.Q);
-    fill(t.cd, t.camPos, t.M, t.a, t.Q);
+    fill(t.cf, t, t.camPos, t.M, t.a, t.Q);
+    fill(t.cd, t, t.camPos, t.M, t.a, t.Q);
 }

@@ -31,6 +31,7 @@
 // accurate library sincos.
 // ---------------------------------------------------------------------------
 #include "bh_shade.cuh"
+#include "bh_internal.h"
 
 enum { RAY_SKIP = 0, RAY_LIVE = 1, RAY_DONE = 2 };
 
@@ -94,32 +95,16 @@ BH_DEV float capture_radius(const TraceParams& P)
     return (P.rPlus > 1e-6f) ? P.rPlus : 0.05f * P.M;
 }
 
-// sin/cos of th + delta from the anchored pair (s, c) of th.  FP32: angle
-// addition with the Taylor series of sin / cos delta to degree 7 / 6
-// (truncation < 4e-10 for |delta| <= 0.3; the adaptive step keeps a stage's
-// angular advance below 2.2 dPhi <= 0.22); larger deltas fall back to the
-// full polynomial.  FP64: the library sincos.
-BH_DEV void sincos_shift(float th, float s, float c, float delta, float& so, float& co)
+// sin/cos of the polar angle.  FP32: the MUFU pair (absolute error ~4e-7),
+// replaced by the polynomial sincos_polar when |sin| < 1/16, so that sin keeps
+// its relative accuracy near the poles where the equations divide by it.
+// FP64: the library sincos.
+BH_DEV void sincos_theta(float x, float& s, float& c)
 {
-    if (fabsf(delta) > 0.3f)
-    {
-        sincos_polar(th + delta, so, co);
-        return;
-    }
-    float d2 = delta * delta;
-    float ps = fmaf(d2, -1.98412698412698413e-4f, 8.33333333333333333e-3f);
-    ps = fmaf(d2, ps, -1.66666666666666667e-1f);
-    float sd = fmaf(delta * d2, ps, delta);
-    float pc = fmaf(d2, -1.38888888888888889e-3f, 4.16666666666666667e-2f);
-    pc = fmaf(d2, pc, -0.5f);
-    float cd = fmaf(d2, pc, 1.f);
-    so = fmaf(s, cd, c * sd);
-    co = fmaf(c, cd, -(s * sd));
+    __sincosf(x, &s, &c);
+    if (fabsf(s) < 0.0625f) sincos_polar(x, s, c);
 }
-BH_DEV void sincos_shift(double th, double, double, double delta, double& so, double& co)
-{
-    sincos(th + delta, &so, &co);
-}
+BH_DEV void sincos_theta(double x, double& s, double& c) { sincos(x, &s, &c); }
 
 // ===========================================================================
 // Spherically symmetric metrics (Schwarzschild, Reissner-Nordstrom)
@@ -198,13 +183,13 @@ struct SphRay
     // the ray has terminated.
     BH_DEV bool advance(const TraceParams& P)
     {
-        const R M = (R)P.M, Q2 = (R)P.Q * (R)P.Q, dPhi = (R)P.dPhi;
+        const CamFrame<R>& F = frame_of<R>(P);
         if (step >= P.maxSteps) { exhaust(P); return true; }
+        const R M = F.M, Q2 = F.Q2, dPhi = F.dPhi;
 
-        const R invNineM = R(1) / (R(9) * M);
-        R hMax = dPhi * min_p(max_p(invNineM * rcp_p(u), R(1)), R(6));
+        R hMax = dPhi * min_p(max_p(F.invNineM * rcp_p(u), R(1)), R(6));
         R h = min_p(hMax, R(0.10f) * rcp_p(max_p(abs_p(du), R(1e-6f))));
-        h = max_p(h, dPhi * R(0.03f));
+        h = max_p(h, F.hMin);
 
         const R m3 = R(3) * M, q2 = R(2) * Q2;
         auto acc = [&](R x) { return (m3 * x - q2 * x * x) * x - x; };
@@ -221,9 +206,8 @@ struct SphRay
         du += h6 * (k1v + R(2) * k2v + R(2) * k3v + k4v);
         phi += h;
 
-        const R uHor = R(1) / max_p((R)capture_radius(P), R(1e-6f));
         if (!finite_p(u) || !finite_p(du)) { horizon = true; return true; }
-        if (u >= uHor) { horizon = true; return true; }
+        if (u >= F.uHor) { horizon = true; return true; }
         if (u < R(1e-4f)) { escaped = true; return true; }   // previous chord direction
 
         R r = rcp_p(u);
@@ -233,25 +217,21 @@ struct SphRay
 
         if (P.diskOn && trans > 0.01f)
         {
-            const CamFrame<R>& F = frame_of<R>(P);
             R sp, cp;
             sincos_fast(phi, sp, cp);
             f3 pos = v3((float)((F.e1[0] * cp + e2x * sp) * r), (float)((F.e1[1] * cp + e2y * sp) * r),
                         (float)((F.e1[2] * cp + e2z * sp) * r));
-            disk_segment<STATS>(P, E, Lz, prevPos, pos, (float)((R)P.diskTime - tFlight),
-                                accum, trans, tally);
+            disk_segment<STATS>(P, E, Lz, prevPos, pos, (float)(F.diskTime - tFlight), accum, trans, tally);
             prevPos = pos;
         }
         ++step;
-        const R uEscape = R(1) / (R(120) * M);
-        if (u < uEscape && du < R(0)) { escaped = true; return true; }
+        if (u < F.uEscape && du < R(0)) { escaped = true; return true; }
         return false;
     }
 
     BH_DEV void exhaust(const TraceParams& P)
     {   // budget spent: reference src/trace.cuh:603-609
-        const R M = (R)P.M;
-        if (u > R(1) / max_p(R(1.5f) * (R)P.rPhoton, R(3) * M)) horizon = true;
+        if (u > frame_of<R>(P).uPh) horizon = true;
         else escaped = true;
     }
 
@@ -296,14 +276,24 @@ struct KerrDeriv { R r, th, ph, pr, pth; };
 
 // Right-hand side of the first-order system plus the constraint K = 2 Sigma H
 // (reference src/trace.cuh:620-659).  s, c: sin/cos of th (s unclamped).
+// Also returns the pieces the slow-light term at the same point reuses.
 template <class R>
-BH_DEV KerrDeriv<R> kerr_rhs(R M, R a, R Q2, R E, R Lz, R r, R s, R c, R pr, R pth, R& K)
+struct KerrEval
 {
+    KerrDeriv<R> d;
+    R K, Pp, iDelT, iS;   // iDelT: 1 / max(Delta, 1e-5), the slow-light clamp
+};
+
+template <class R>
+BH_DEV KerrEval<R> kerr_rhs(const CamFrame<R>& F, R E, R Lz, R r, R s, R c, R pr, R pth)
+{
+    const R M = F.M, a = F.a, a2 = F.a2;
     s = max_p(s, R(1e-4f));                 // pole guard
-    const R a2 = a * a, aE = a * E;
+    const R aE = a * E;
     R r2 = r * r;
     R Sig = r2 + a2 * c * c;
-    R Del = max_p(r2 - R(2) * M * r + a2 + Q2, R(1e-6f));
+    R DelRaw = r2 - R(2) * M * r + a2 + F.Q2;
+    R Del = max_p(DelRaw, R(1e-6f));
     R Pp = E * (r2 + a2) - a * Lz;
     R is = rcp_p(s);
     R is2 = is * is;
@@ -311,20 +301,23 @@ BH_DEV KerrDeriv<R> kerr_rhs(R M, R a, R Q2, R E, R Lz, R r, R s, R c, R pr, R p
     R iDel = rcp_p(Del);
     R PiD = Pp * iDel;
     R W = B * B - Pp * PiD;
-    K = Del * pr * pr + pth * pth + W;
+    KerrEval<R> o;
+    o.K = Del * pr * pr + pth * pth + W;
     R dDel = R(2) * r - R(2) * M;
     R dP = R(2) * r * E;
     R Wr = -PiD * (R(2) * dP - PiD * dDel);
     R Wth = R(2) * B * (-c * (Lz * is2 + aE));
     R iS = rcp_p(Sig);
     R iS2 = iS * iS;
-    KerrDeriv<R> d;
-    d.r = Del * pr * iS;
-    d.th = pth * iS;
-    d.ph = ((Lz * is2 - aE) + a * PiD) * iS;
-    d.pr = R(-0.5f) * iS * (dDel * pr * pr + Wr) + r * iS2 * K;
-    d.pth = R(-0.5f) * iS * Wth - a2 * s * c * iS2 * K;
-    return d;
+    o.d.r = Del * pr * iS;
+    o.d.th = pth * iS;
+    o.d.ph = ((Lz * is2 - aE) + a * PiD) * iS;
+    o.d.pr = R(-0.5f) * iS * (dDel * pr * pr + Wr) + r * iS2 * o.K;
+    o.d.pth = R(-0.5f) * iS * Wth - a2 * s * c * iS2 * o.K;
+    o.Pp = Pp;
+    o.iDelT = (DelRaw >= R(1e-5f)) ? iDel : R(1e5f);
+    o.iS = iS;
+    return o;
 }
 
 template <class R, bool STATS>
@@ -332,15 +325,24 @@ struct KerrRay
 {
     using Real = R;
     R r, th, ph, pr, pth;   // Boyer-Lindquist state
-    R s, c;                 // sin/cos of th, carried between steps
+    R s, c;                 // sin/cos of th
     R E, Lz, tFlight;
-    R dr_, dth_, dph_;      // coordinate derivative that defines the escape direction
+    KerrDeriv<R> d1;        // right-hand side at the current state
+    R K1;
     f3 prevPos, accum;
     float trans, maxHviol;
     int step;
     bool horizon, escaped, useDeriv;
     DiskTally tally;
     double Q0;
+
+    // the reference's dLast (derivative of the final RK4 stage), kept only on
+    // the last step the budget allows: it is needed only if that budget runs out
+    BH_DEV static R* last_deriv()
+    {
+        __shared__ R dl[BH_TRACE_BLOCK][3];
+        return dl[threadIdx.x];
+    }
 
     BH_DEV int init(const TraceParams& P, f3 dirf)
     {   // reference src/trace.cuh:703-739: the per-ray remainder of the tetrad map
@@ -354,7 +356,10 @@ struct KerrRay
         r = F.r0; th = F.th0; ph = F.ph0;
         pr = xmul(drc, F.sqSD);
         pth = xmul(dtc, F.sqS);
-        sincos_polar(th, s, c);
+        sincos_theta(th, s, c);
+        KerrEval<R> ev = kerr_rhs(F, E, Lz, r, s, c, pr, pth);
+        d1 = ev.d;
+        K1 = ev.K;
 
         tFlight = R(0);
         prevPos = tof3(P.camPos);
@@ -363,11 +368,10 @@ struct KerrRay
         maxHviol = 0.f;
         step = 0;
         horizon = escaped = useDeriv = false;
-        dr_ = dth_ = dph_ = R(0);
         if (STATS)
         {
             tally.samples = 0; tally.hitR = 0.f; tally.hitG = 0.f;
-            Q0 = carterQ(th, pth, (R)P.a, E, Lz);
+            Q0 = carterQ(th, pth, F.a, E, Lz);
         }
         return RAY_LIVE;
     }
@@ -381,62 +385,52 @@ struct KerrRay
         return (double)pth_ * pth_ + cd * cd * ((double)Lz_ * Lz_ / s2 - (double)a * a * (double)E_ * E_);
     }
 
-    // One reference loop iteration (src/trace.cuh:752-868).  Returns true when
-    // the ray has terminated.
+    // One reference loop iteration (src/trace.cuh:752-868).  The first
+    // right-hand side of the step (d1) was evaluated at the end of the previous
+    // iteration, where its Sigma, Delta and P also gave the slow-light term.
+    // Returns true when the ray has terminated.
     BH_DEV bool advance(const TraceParams& P)
     {
+        const CamFrame<R>& F = frame_of<R>(P);
         if (step >= P.maxSteps) { exhaust(P); return true; }
-        const R M = (R)P.M, a = (R)P.a, Q2 = (R)P.Q * (R)P.Q;
-        const R dPhi = (R)P.dPhi;
-        const R rCap = (R)capture_radius(P);
-        const R rFloor = max_p((R)P.rPlus, rCap);
-
-        R K1;
-        KerrDeriv<R> d1 = kerr_rhs(M, a, Q2, E, Lz, r, s, c, pr, pth, K1);
         if (!finite_p(r) || !finite_p(pr) || !finite_p(pth) || !finite_p(d1.r) || !finite_p(d1.pr))
         { horizon = true; return true; }
-        if (r <= rCap * R(1.002f) + R(1e-3f)) { horizon = true; return true; }
-        if (STATS && r > rFloor * R(1.05f))
+        if (r <= F.capR) { horizon = true; return true; }
+        if (STATS && r > F.rFloor105)
         {
-            float viol = (float)(abs_p(K1) / (E * E * (r * r + a * a) + R(1e-12f)));
+            float viol = (float)(abs_p(K1) / (E * E * (r * r + F.a2) + R(1e-12f)));
             maxHviol = fmaxf(maxHviol, viol);
         }
-        if (r >= R(120) * M && d1.r > R(0))
-        {
-            dr_ = d1.r; dth_ = d1.th; dph_ = d1.ph;
-            escaped = useDeriv = true;
-            return true;
-        }
+        if (r >= F.escR && d1.r > R(0)) { escaped = useDeriv = true; return true; }
 
         // adaptive affine step (reference src/trace.cuh:793-809)
-        const R i8 = rcp_p(R(8.0f) * dPhi * max_p(r - rFloor, R(0.02f)));
         const R ang = abs_p(d1.th) + abs_p(d1.ph);
-        R h = rcp_p(abs_p(d1.r) * i8 + ang * rcp_p(R(2.2f) * dPhi) + R(1e-5f));
-        if (r < R(1.5f) * (R)P.rPhoton) h *= R(0.55f);
+        R h = rcp_p(abs_p(d1.r) * rcp_p(F.k8dPhi * max_p(r - F.rFloor, R(0.02f))) + ang * F.i22dPhi + R(1e-5f));
+        if (r < F.rPh15) h *= R(0.55f);
         R spd = abs_p(d1.r) + r * ang + R(1e-6f);
         R capLen;
-        if (P.diskOn && r < (R)P.diskOuter * R(1.3f))
+        if (P.diskOn && r < F.outer13)
             capLen = (r * abs_p(c) < R(1.8f)) ? R(1.2f) : R(2.2f);
         else
             capLen = max_p(R(1.2f), R(0.22f) * r);
         h = min_p(h, capLen * rcp_p(spd));
 
-        // classic RK4; stage angles th + delta via angle addition from (s, c)
+        // classic RK4
         const R hh = R(0.5f) * h;
-        R Kx, sx, cx;
-        R yr = r + hh * d1.r, ypr = pr + hh * d1.pr, ypth = pth + hh * d1.pth;
-        sincos_shift(th, s, c, hh * d1.th, sx, cx);
-        KerrDeriv<R> d2 = kerr_rhs(M, a, Q2, E, Lz, yr, sx, cx, ypr, ypth, Kx);
+        R sx, cx;
+        R yr = r + hh * d1.r, yth = th + hh * d1.th, ypr = pr + hh * d1.pr, ypth = pth + hh * d1.pth;
+        sincos_theta(yth, sx, cx);
+        KerrDeriv<R> d2 = kerr_rhs(F, E, Lz, yr, sx, cx, ypr, ypth).d;
         R sr = d1.r + R(2) * d2.r, sth = d1.th + R(2) * d2.th, sph = d1.ph + R(2) * d2.ph;
         R spr = d1.pr + R(2) * d2.pr, spth = d1.pth + R(2) * d2.pth;
-        yr = r + hh * d2.r; ypr = pr + hh * d2.pr; ypth = pth + hh * d2.pth;
-        sincos_shift(th, s, c, hh * d2.th, sx, cx);
-        KerrDeriv<R> d3 = kerr_rhs(M, a, Q2, E, Lz, yr, sx, cx, ypr, ypth, Kx);
+        yr = r + hh * d2.r; yth = th + hh * d2.th; ypr = pr + hh * d2.pr; ypth = pth + hh * d2.pth;
+        sincos_theta(yth, sx, cx);
+        KerrDeriv<R> d3 = kerr_rhs(F, E, Lz, yr, sx, cx, ypr, ypth).d;
         sr += R(2) * d3.r; sth += R(2) * d3.th; sph += R(2) * d3.ph;
         spr += R(2) * d3.pr; spth += R(2) * d3.pth;
-        yr = r + h * d3.r; ypr = pr + h * d3.pr; ypth = pth + h * d3.pth;
-        sincos_shift(th, s, c, h * d3.th, sx, cx);
-        KerrDeriv<R> d4 = kerr_rhs(M, a, Q2, E, Lz, yr, sx, cx, ypr, ypth, Kx);
+        yr = r + h * d3.r; yth = th + h * d3.th; ypr = pr + h * d3.pr; ypth = pth + h * d3.pth;
+        sincos_theta(yth, sx, cx);
+        KerrDeriv<R> d4 = kerr_rhs(F, E, Lz, yr, sx, cx, ypr, ypth).d;
         const R h6 = h * R(1.0 / 6.0);
         r += h6 * (sr + d4.r);
         th += h6 * (sth + d4.th);
@@ -447,16 +441,22 @@ struct KerrRay
         // pole reflection guard
         if (th < R(1e-3f)) { th = R(1e-3f); pth = abs_p(pth); }
         else if (th > R(kPiF - 1e-3f)) { th = R(kPiF - 1e-3f); pth = -abs_p(pth); }
-        dr_ = d4.r; dth_ = d4.th; dph_ = d4.ph;   // dLast of the reference
-        sincos_polar(th, s, c);
+        ++step;
+        if (step == P.maxSteps)
+        {
+            R* dl = last_deriv();
+            dl[0] = d4.r; dl[1] = d4.th; dl[2] = d4.ph;
+        }
 
-        {   // slow light: Sigma dt/dl = a (Lz - a E sin^2) + (r^2 + a^2) P / Delta
-            R sc = max_p(s, R(1e-4f));
-            R r2a2 = r * r + a * a;
-            R Sig = r * r + a * a * c * c;
-            R Del = max_p(r * r - R(2) * M * r + a * a + Q2, R(1e-5f));
-            R Pp = E * r2a2 - a * Lz;
-            R dtdl = (a * (Lz - a * E * sc * sc) + r2a2 * Pp * rcp_p(Del)) * rcp_p(max_p(Sig, R(1e-8f)));
+        // next step's first right-hand side; its Sigma, Delta, P give the slow
+        // light  Sigma dt/dl = a (Lz - a E sin^2) + (r^2 + a^2) P / Delta
+        sincos_theta(th, s, c);
+        KerrEval<R> ev = kerr_rhs(F, E, Lz, r, s, c, pr, pth);
+        d1 = ev.d;
+        K1 = ev.K;
+        {
+            const R sc = max_p(s, R(1e-4f));
+            const R dtdl = (F.a * (Lz - F.a * E * sc * sc) + (r * r + F.a2) * ev.Pp * ev.iDelT) * ev.iS;
             tFlight += h * abs_p(dtdl);
         }
         if (P.diskOn)
@@ -465,17 +465,16 @@ struct KerrRay
             sincos_fast(ph, sp, cp);
             f3 pos = v3((float)(r * s * cp), (float)(r * c), (float)(-r * s * sp));
             if (trans > 0.01f)
-                disk_segment<STATS>(P, (float)E, (float)Lz, prevPos, pos,
-                                    (float)((R)P.diskTime - tFlight), accum, trans, tally);
+                disk_segment<STATS>(P, (float)E, (float)Lz, prevPos, pos, (float)(F.diskTime - tFlight),
+                                    accum, trans, tally);
             prevPos = pos;
         }
-        ++step;
         return false;
     }
 
     BH_DEV void exhaust(const TraceParams& P)
     {   // budget spent: reference src/trace.cuh:871-888
-        if (r < R(6) * (R)P.M) horizon = true;
+        if (r < frame_of<R>(P).sixM) horizon = true;
         else { escaped = true; useDeriv = step > 0; }
     }
 
@@ -485,7 +484,13 @@ struct KerrRay
         q.key = key | (horizon ? kRayHorizon : 0u) | (escaped ? kRayEscaped : 0u) | (useState ? kRayUseState : 0u);
         q.acc[0] = accum.x; q.acc[1] = accum.y; q.acc[2] = accum.z;
         q.trans = trans;
-        q.f[0] = r; q.f[1] = th; q.f[2] = ph; q.f[3] = dr_; q.f[4] = dth_; q.f[5] = dph_;
+        q.f[0] = r; q.f[1] = th; q.f[2] = ph;
+        if (useState && step >= P.maxSteps)
+        {   // budget exhausted: the derivative of the last RK4 stage
+            const R* dl = last_deriv();
+            q.f[3] = dl[0]; q.f[4] = dl[1]; q.f[5] = dl[2];
+        }
+        else { q.f[3] = d1.r; q.f[4] = d1.th; q.f[5] = d1.ph; }
         if (STATS)
         {
             st->steps = step; st->samples = tally.samples; st->maxHviol = maxHviol;

@@ -8,6 +8,11 @@
 #include "bh_trace_params.h"
 
 #define BH_TRACE_BLOCK 128
+// resident CTAs per SM the tracing kernels are register-budgeted for
+// (65536 / (128 * 7) -> 72 registers per thread, 28 warps per SM)
+#ifndef BH_TRACE_MIN_BLOCKS
+#define BH_TRACE_MIN_BLOCKS 7
+#endif
 
 struct PostConsts
 {

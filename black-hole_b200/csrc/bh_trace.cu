@@ -121,7 +121,7 @@ BH_DEV void shade_slot(const TraceParams& P, const PackedRay<typename Ray::Real>
 }
 
 template <class Ray, bool STATS>
-__global__ void __launch_bounds__(BH_TRACE_BLOCK)
+__global__ void __launch_bounds__(BH_TRACE_BLOCK, BH_TRACE_MIN_BLOCKS)
 trace_kernel(const __grid_constant__ TraceParams P)
 {
     using R = typename Ray::Real;
@@ -187,7 +187,10 @@ trace_kernel(const __grid_constant__ TraceParams P)
             break;   // no rays left for this warp
         }
 
-        if (live && ray.advance(P)) { live = false; fin = true; }
+        // two steps per scheduling round: halves the ballot / refill bookkeeping
+#pragma unroll 1
+        for (int k = 0; k < 2; ++k)
+            if (live && ray.advance(P)) { live = false; fin = true; }
 
         const unsigned finMask = __ballot_sync(FULL, fin);
         if (finMask)

@@ -38,6 +38,18 @@ struct CamFrame
     T gttS, gtpS, gppS, AS, rsqS;
     T f0, sf0, u0;               // max(f(r0), 1e-6), sqrt(f0), 1/r0
     int camAtOrigin;             // r0 < 1e-4: E = 1, Lz = 0
+
+    // step-loop constants (the reference's expressions, evaluated once)
+    T M, a, Q2, a2;
+    T capR;                      // capture test r <= rCap * 1.002 + 1e-3
+    T rFloor, rFloor105;         // max(r+, rCap), and x 1.05 (constraint monitor)
+    T escR, sixM;                // 120 M, 6 M
+    T k8dPhi, i22dPhi;           // 8 dPhi, 1 / (2.2 dPhi)
+    T rPh15, outer13;            // 1.5 r_photon, 1.3 diskOuter
+    T dPhi, hMin;                // dPhi, 0.03 dPhi (spherical step floor)
+    T uHor, uEscape, invNineM;   // 1/max(rCap, 1e-6), 1/(120 M), 1/(9 M)
+    T uPh;                       // 1 / max(1.5 r_photon, 3 M)
+    T diskTime;
 };
 
 struct TraceParams
