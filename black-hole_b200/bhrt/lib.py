@@ -32,6 +32,7 @@ _SIGNATURES = {
     "bhPostProcess": (_int, [_vp, _vp, _vp, _vp, _P, _vp]),
     "bhSetTuning": (_int, [_int, _int, _int]),
     "bhGetTuning": (None, [_int, C.POINTER(_int), C.POINTER(_int)]),
+    "bhSetTileOrder": (_int, [_int]),
     "bhMeasureFp32Peak": (C.c_double, []),
     "bhVersion": (C.c_char_p, []),
 }

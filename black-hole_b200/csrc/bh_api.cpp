@@ -8,8 +8,10 @@
 // the launch status, as in the reference launchers
 // (src/black_hole_kernel.cu:108-163 of Sqhh99/Black-hole).
 // ---------------------------------------------------------------------------
+#include <algorithm>
 #include <cmath>
 #include <mutex>
+#include <vector>
 #include <cuda_runtime.h>
 #include "bh_launch.h"
 #include "bh_internal.h"
@@ -37,6 +39,65 @@ cudaError_t deviceScratch(unsigned** out)
         gScratch[dev] = static_cast<unsigned*>(p);
     }
     *out = gScratch[dev];
+    return cudaSuccess;
+}
+
+// ---- trace order of the 8x4 tiles ---------------------------------------------------
+// Mode 1 (centre-out) traces tiles in order of distance from the image centre:
+// with the hole at the centre of the view, the shadow and photon ring -- the
+// longest rays -- go first and the frame's last tiles are short escaping rays,
+// which shortens the tail where SMs run out of work.  The table depends only on
+// the resolution; it is built and uploaded once per device and resolution.
+struct OrderCache
+{
+    int W = 0, H = 0;
+    unsigned* dev = nullptr;
+    size_t cap = 0;
+};
+OrderCache gOrder[kMaxDevices];
+int gTileOrderMode = 1;
+
+cudaError_t tileOrder(int W, int H, const unsigned** out)
+{
+    *out = nullptr;
+    if (gTileOrderMode == 0) return cudaSuccess;
+    int dev = 0;
+    cudaError_t e = cudaGetDevice(&dev);
+    if (e != cudaSuccess) return e;
+    if (dev < 0 || dev >= kMaxDevices) return cudaErrorInvalidDevice;
+    std::lock_guard<std::mutex> g(gScratchLock);
+    OrderCache& c = gOrder[dev];
+    if (c.W != W || c.H != H || !c.dev)
+    {
+        const int tx = (W + 7) / 8, ty = (H + 3) / 4;
+        const size_t n = (size_t)tx * ty;
+        std::vector<unsigned> order(n);
+        std::vector<float> key(n);
+        const float cx = 0.5f * W, cy = 0.5f * H;
+        for (size_t i = 0; i < n; ++i)
+        {
+            order[i] = (unsigned)i;
+            const float dx = ((float)(i % tx) * 8.f + 4.f) - cx, dy = ((float)(i / tx) * 4.f + 2.f) - cy;
+            key[i] = dx * dx + dy * dy;
+        }
+        std::stable_sort(order.begin(), order.end(), [&](unsigned a, unsigned b) { return key[a] < key[b]; });
+        if (c.cap < n)
+        {
+            if (c.dev) cudaFree(c.dev);
+            c.dev = nullptr;
+            c.cap = 0;
+            void* p = nullptr;
+            e = cudaMalloc(&p, n * sizeof(unsigned));
+            if (e != cudaSuccess) return e;
+            c.dev = static_cast<unsigned*>(p);
+            c.cap = n;
+        }
+        e = cudaMemcpy(c.dev, order.data(), n * sizeof(unsigned), cudaMemcpyHostToDevice);
+        if (e != cudaSuccess) return e;
+        c.W = W;
+        c.H = H;
+    }
+    *out = c.dev;
     return cudaSuccess;
 }
 
@@ -128,6 +189,11 @@ cudaError_t trace(TraceParams t, const RenderParams& P, int precision, bool stat
     if (!t.out) return cudaErrorInvalidValue;
     cudaError_t e = deviceScratch(&t.counter);
     if (e != cudaSuccess) return e;
+    if (!t.dirs)
+    {
+        e = tileOrder(t.W, t.H, &t.tileOrder);
+        if (e != cudaSuccess) return e;
+    }
     return bh_launch_trace(t, precision, stats, familyBlocks(P), s);
 }
 
@@ -225,6 +291,13 @@ int bhSetTuning(int family, int refillMin, int blocksPerSm)
     if (family < 0 || family > 1 || refillMin < 1 || refillMin > 32 || blocksPerSm < 0) return 0;
     gTune[family].refillMin = refillMin;
     gTune[family].blocksPerSm = blocksPerSm;
+    return 1;
+}
+
+int bhSetTileOrder(int mode)
+{
+    if (mode < 0 || mode > 1) return 0;
+    gTileOrderMode = mode;
     return 1;
 }
 

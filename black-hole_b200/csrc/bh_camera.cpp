@@ -92,7 +92,7 @@ void fill(CamFrame<T>& f, const TraceParams& t, float3 pos, float Mf, float af, 
 
     // ---- step-loop constants: trace.cuh:477-482, 537, 548-550, 607, 696-701, 761-808, 874
     const T rCap = (T)t.rCap, dPhi = (T)t.dPhi;
-    f.M = M; f.a = a; f.Q2 = Q * Q; f.a2 = a * a;
+    f.M = M; f.a = a; f.Q2 = Q * Q; f.a2 = a * a; f.a2Q2 = f.a2 + f.Q2;
     f.capR = rCap * T(1.002f) + T(1e-3f);
     f.rFloor = fmaxT((T)t.rPlus, rCap);
     f.rFloor105 = f.rFloor * T(1.05f);

@@ -106,6 +106,12 @@ BH_DEV void sincos_theta(float x, float& s, float& c)
 }
 BH_DEV void sincos_theta(double x, double& s, double& c) { sincos(x, &s, &c); }
 
+// RK4 stage angles: the plain MUFU pair in FP32.  A stage only feeds the step
+// update with weight h/6..h/3, and the state's own sin/cos (sincos_theta) keeps
+// the relative accuracy at the poles.
+BH_DEV void sincos_stage(float x, float& s, float& c) { __sincosf(x, &s, &c); }
+BH_DEV void sincos_stage(double x, double& s, double& c) { sincos(x, &s, &c); }
+
 // ===========================================================================
 // Spherically symmetric metrics (Schwarzschild, Reissner-Nordstrom)
 // ===========================================================================
@@ -284,36 +290,44 @@ struct KerrEval
     R K, Pp, iDelT, iS;   // iDelT: 1 / max(Delta, 1e-5), the slow-light clamp
 };
 
+// Per-ray constants of the right-hand side: products of E, Lz, a that the
+// reference recomputes at every evaluation.
 template <class R>
-BH_DEV KerrEval<R> kerr_rhs(const CamFrame<R>& F, R E, R Lz, R r, R s, R c, R pr, R pth)
+struct KerrConsts
 {
-    const R M = F.M, a = F.a, a2 = F.a2;
+    R E, Lz, aE, c1, twoE;   // c1 = E a^2 - a Lz, so P = E r^2 + c1
+};
+
+template <class R>
+BH_DEV KerrEval<R> kerr_rhs(const CamFrame<R>& F, const KerrConsts<R>& k, R r, R s, R c, R pr, R pth)
+{
+    const R M = F.M, a2 = F.a2;
     s = max_p(s, R(1e-4f));                 // pole guard
-    const R aE = a * E;
     R r2 = r * r;
     R Sig = r2 + a2 * c * c;
-    R DelRaw = r2 - R(2) * M * r + a2 + F.Q2;
+    R DelRaw = r * (r - R(2) * M) + F.a2Q2;
     R Del = max_p(DelRaw, R(1e-6f));
-    R Pp = E * (r2 + a2) - a * Lz;
+    R Pp = k.E * r2 + k.c1;                 // E (r^2 + a^2) - a Lz
     R is = rcp_p(s);
     R is2 = is * is;
-    R B = Lz * is - aE * s;
+    R B = k.Lz * is - k.aE * s;
     R iDel = rcp_p(Del);
     R PiD = Pp * iDel;
     R W = B * B - Pp * PiD;
     KerrEval<R> o;
     o.K = Del * pr * pr + pth * pth + W;
-    R dDel = R(2) * r - R(2) * M;
-    R dP = R(2) * r * E;
-    R Wr = -PiD * (R(2) * dP - PiD * dDel);
-    R Wth = R(2) * B * (-c * (Lz * is2 + aE));
+    R dDel = R(2) * (r - M);
+    R Wr = -PiD * (R(2) * k.twoE * r - PiD * dDel);   // dP = 2 r E
+    R Wth = R(-2) * B * c * (k.Lz * is2 + k.aE);
     R iS = rcp_p(Sig);
     R iS2 = iS * iS;
+    R mh = R(-0.5f) * iS;
+    R KiS2 = o.K * iS2;
     o.d.r = Del * pr * iS;
     o.d.th = pth * iS;
-    o.d.ph = ((Lz * is2 - aE) + a * PiD) * iS;
-    o.d.pr = R(-0.5f) * iS * (dDel * pr * pr + Wr) + r * iS2 * o.K;
-    o.d.pth = R(-0.5f) * iS * Wth - a2 * s * c * iS2 * o.K;
+    o.d.ph = ((k.Lz * is2 - k.aE) + F.a * PiD) * iS;
+    o.d.pr = mh * (dDel * pr * pr + Wr) + r * KiS2;
+    o.d.pth = mh * Wth - a2 * s * c * KiS2;
     o.Pp = Pp;
     o.iDelT = (DelRaw >= R(1e-5f)) ? iDel : R(1e5f);
     o.iS = iS;
@@ -326,7 +340,8 @@ struct KerrRay
     using Real = R;
     R r, th, ph, pr, pth;   // Boyer-Lindquist state
     R s, c;                 // sin/cos of th
-    R E, Lz, tFlight;
+    KerrConsts<R> k;        // E, Lz and their products
+    R tFlight;
     KerrDeriv<R> d1;        // right-hand side at the current state
     R K1;
     f3 prevPos, accum;
@@ -351,13 +366,14 @@ struct KerrRay
         R drc = xdot(F.er, dir), dtc = xdot(F.eth, dir), dpc = xdot(F.eph, dir);
         R ptUp = xsub(F.rsq, xdiv(xmul(xmul(dpc, F.A), F.gtp), F.gtt));
         R pfUp = xmul(dpc, F.A);
-        E = -xadd(xmul(F.gtt, ptUp), xmul(F.gtp, pfUp));
-        Lz = xadd(xmul(F.gtp, ptUp), xmul(F.gpp, pfUp));
+        const R E = -xadd(xmul(F.gtt, ptUp), xmul(F.gtp, pfUp));
+        const R Lz = xadd(xmul(F.gtp, ptUp), xmul(F.gpp, pfUp));
+        k.E = E; k.Lz = Lz; k.aE = F.a * E; k.c1 = E * F.a2 - F.a * Lz; k.twoE = R(2) * E;
         r = F.r0; th = F.th0; ph = F.ph0;
         pr = xmul(drc, F.sqSD);
         pth = xmul(dtc, F.sqS);
         sincos_theta(th, s, c);
-        KerrEval<R> ev = kerr_rhs(F, E, Lz, r, s, c, pr, pth);
+        KerrEval<R> ev = kerr_rhs(F, k, r, s, c, pr, pth);
         d1 = ev.d;
         K1 = ev.K;
 
@@ -398,7 +414,7 @@ struct KerrRay
         if (r <= F.capR) { horizon = true; return true; }
         if (STATS && r > F.rFloor105)
         {
-            float viol = (float)(abs_p(K1) / (E * E * (r * r + F.a2) + R(1e-12f)));
+            float viol = (float)(abs_p(K1) / (k.E * k.E * (r * r + F.a2) + R(1e-12f)));
             maxHviol = fmaxf(maxHviol, viol);
         }
         if (r >= F.escR && d1.r > R(0)) { escaped = useDeriv = true; return true; }
@@ -419,18 +435,18 @@ struct KerrRay
         const R hh = R(0.5f) * h;
         R sx, cx;
         R yr = r + hh * d1.r, yth = th + hh * d1.th, ypr = pr + hh * d1.pr, ypth = pth + hh * d1.pth;
-        sincos_theta(yth, sx, cx);
-        KerrDeriv<R> d2 = kerr_rhs(F, E, Lz, yr, sx, cx, ypr, ypth).d;
+        sincos_stage(yth, sx, cx);
+        KerrDeriv<R> d2 = kerr_rhs(F, k, yr, sx, cx, ypr, ypth).d;
         R sr = d1.r + R(2) * d2.r, sth = d1.th + R(2) * d2.th, sph = d1.ph + R(2) * d2.ph;
         R spr = d1.pr + R(2) * d2.pr, spth = d1.pth + R(2) * d2.pth;
         yr = r + hh * d2.r; yth = th + hh * d2.th; ypr = pr + hh * d2.pr; ypth = pth + hh * d2.pth;
-        sincos_theta(yth, sx, cx);
-        KerrDeriv<R> d3 = kerr_rhs(F, E, Lz, yr, sx, cx, ypr, ypth).d;
+        sincos_stage(yth, sx, cx);
+        KerrDeriv<R> d3 = kerr_rhs(F, k, yr, sx, cx, ypr, ypth).d;
         sr += R(2) * d3.r; sth += R(2) * d3.th; sph += R(2) * d3.ph;
         spr += R(2) * d3.pr; spth += R(2) * d3.pth;
         yr = r + h * d3.r; yth = th + h * d3.th; ypr = pr + h * d3.pr; ypth = pth + h * d3.pth;
-        sincos_theta(yth, sx, cx);
-        KerrDeriv<R> d4 = kerr_rhs(F, E, Lz, yr, sx, cx, ypr, ypth).d;
+        sincos_stage(yth, sx, cx);
+        KerrDeriv<R> d4 = kerr_rhs(F, k, yr, sx, cx, ypr, ypth).d;
         const R h6 = h * R(1.0 / 6.0);
         r += h6 * (sr + d4.r);
         th += h6 * (sth + d4.th);
@@ -451,12 +467,12 @@ struct KerrRay
         // next step's first right-hand side; its Sigma, Delta, P give the slow
         // light  Sigma dt/dl = a (Lz - a E sin^2) + (r^2 + a^2) P / Delta
         sincos_theta(th, s, c);
-        KerrEval<R> ev = kerr_rhs(F, E, Lz, r, s, c, pr, pth);
+        KerrEval<R> ev = kerr_rhs(F, k, r, s, c, pr, pth);
         d1 = ev.d;
         K1 = ev.K;
         {
             const R sc = max_p(s, R(1e-4f));
-            const R dtdl = (F.a * (Lz - F.a * E * sc * sc) + (r * r + F.a2) * ev.Pp * ev.iDelT) * ev.iS;
+            const R dtdl = (F.a * (k.Lz - k.aE * sc * sc) + (r * r + F.a2) * ev.Pp * ev.iDelT) * ev.iS;
             tFlight += h * abs_p(dtdl);
         }
         if (P.diskOn)
@@ -465,7 +481,7 @@ struct KerrRay
             sincos_fast(ph, sp, cp);
             f3 pos = v3((float)(r * s * cp), (float)(r * c), (float)(-r * s * sp));
             if (trans > 0.01f)
-                disk_segment<STATS>(P, (float)E, (float)Lz, prevPos, pos, (float)(F.diskTime - tFlight),
+                disk_segment<STATS>(P, (float)k.E, (float)k.Lz, prevPos, pos, (float)(F.diskTime - tFlight),
                                     accum, trans, tally);
             prevPos = pos;
         }
@@ -496,8 +512,8 @@ struct KerrRay
             st->steps = step; st->samples = tally.samples; st->maxHviol = maxHviol;
             st->hitR = tally.hitR; st->hitG = tally.hitG;
             const R a = (R)P.a;
-            double q1 = carterQ(th, pth, a, E, Lz);
-            double scale = fabs(Q0) + (double)Lz * Lz + (double)a * a * (double)E * E;
+            double q1 = carterQ(th, pth, a, k.E, k.Lz);
+            double scale = fabs(Q0) + (double)k.Lz * k.Lz + (double)a * a * (double)k.E * k.E;
             st->drift = scale > 0.0 ? (float)(fabs(q1 - Q0) / scale) : 0.f;
         }
     }

@@ -17,6 +17,9 @@
 #include <math_constants.h>
 
 #define BH_DEV __device__ __forceinline__
+// Large shading routines called from several places stay out of line: one
+// copy in the kernel keeps the hot step loop's instruction footprint small.
+#define BH_DEV_CALL static __device__ __noinline__
 
 // ---- small vector type ------------------------------------------------------
 template <class T> struct vec3 { T x, y, z; };
@@ -169,7 +172,7 @@ BH_DEV float vnoise(float px, float py)
     return lerp_x(lerp_x(c00, c10, ux), lerp_x(c01, c11, ux), uy);
 }
 
-BH_DEV float fbm3(float px, float py)
+BH_DEV_CALL float fbm3(float px, float py)
 {
     float v = 0.f, amp = 0.5f;
 #pragma unroll

@@ -56,7 +56,7 @@ BH_DEV float thin_disk_flux(float r, float rIn)
 }
 
 // Tanner-Helland blackbody fit, linearised (gamma 2.2).
-BH_DEV f3 blackbody(float kelvin)
+BH_DEV_CALL f3 blackbody(float kelvin)
 {
     float t = clampf(kelvin, 1200.f, 40000.f) * 0.01f;
     float r, g, b;
@@ -75,7 +75,7 @@ BH_DEV f3 blackbody(float kelvin)
 }
 
 // One star population on a cubic lattice of `cell` cells per unit direction.
-BH_DEV f3 star_layer(f3 d, float cell, float intensity, float sharp)
+BH_DEV_CALL f3 star_layer(f3 d, float cell, float intensity, float sharp)
 {
     f3 p = v3(mul_x(d.x, cell), mul_x(d.y, cell), mul_x(d.z, cell));
     f3 id = v3(floorf(p.x), floorf(p.y), floorf(p.z));

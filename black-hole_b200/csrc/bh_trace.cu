@@ -41,6 +41,7 @@ template <class R> struct Queue<R, true> { PackedRay<R> s[kWarps][kQueue]; Packe
 BH_DEV bool ray_pixel(const TraceParams& P, unsigned rid, int& px, int& py)
 {
     unsigned tile = rid >> 5, w = rid & 31u;
+    if (P.tileOrder) tile = __ldg(P.tileOrder + tile);
     px = (int)((tile % (unsigned)P.tilesX) * 8u + (w & 7u));
     py = (int)((tile / (unsigned)P.tilesX) * 4u + (w >> 3));
     return px < P.W && py < P.H;
@@ -120,8 +121,16 @@ BH_DEV void shade_slot(const TraceParams& P, const PackedRay<typename Ray::Real>
     }
 }
 
+// register budget: FP32 render kernels BH_TRACE_MIN_BLOCKS CTAs per SM; the
+// FP64 oracle and the statistics (probe) kernels carry more state, 4 CTAs
 template <class Ray, bool STATS>
-__global__ void __launch_bounds__(BH_TRACE_BLOCK, BH_TRACE_MIN_BLOCKS)
+constexpr int min_blocks()
+{
+    return (sizeof(typename Ray::Real) == 4 && !STATS) ? BH_TRACE_MIN_BLOCKS : 4;
+}
+
+template <class Ray, bool STATS>
+__global__ void __launch_bounds__(BH_TRACE_BLOCK, min_blocks<Ray, STATS>())
 trace_kernel(const __grid_constant__ TraceParams P)
 {
     using R = typename Ray::Real;

@@ -40,7 +40,7 @@ struct CamFrame
     int camAtOrigin;             // r0 < 1e-4: E = 1, Lz = 0
 
     // step-loop constants (the reference's expressions, evaluated once)
-    T M, a, Q2, a2;
+    T M, a, Q2, a2, a2Q2;
     T capR;                      // capture test r <= rCap * 1.002 + 1e-3
     T rFloor, rFloor105;         // max(r+, rCap), and x 1.05 (constraint monitor)
     T escR, sixM;                // 120 M, 6 M
@@ -88,6 +88,7 @@ struct TraceParams
     // work distribution
     unsigned* counter;            // ray counter, zeroed before the launch
     int refillMin;                // refill a warp when at least this many lanes are free
+    const unsigned* tileOrder;    // non-null: k-th claimed tile -> tile index (trace order)
 
     CamFrame<float> cf;           // FP32 integration
     CamFrame<double> cd;          // FP64 integration

@@ -143,6 +143,13 @@ cudaError_t bhPostProcess(uchar4* out, const float4* accum, float4* bloomA, floa
 int bhSetTuning(int family, int refillMin, int blocksPerSm);
 void bhGetTuning(int family, int* refillMin, int* blocksPerSm);
 
+/* Order in which the 8x4-pixel tiles of a frame are traced: 0 row-major,
+ * 1 centre-out (default; the shadow and photon ring first, so the frame ends on
+ * short escaping rays).  The table is built once per device and resolution on
+ * the first call at that resolution (a blocking upload: make that first call
+ * outside any stream capture).  Returns 1 when applied, 0 when out of range. */
+int bhSetTileOrder(int mode);
+
 /* Measured FP32 FMA throughput of the current device, in TFLOP/s, from a
  * dependent-chain FMA kernel timed with CUDA events (blocking). */
 double bhMeasureFp32Peak(void);
