@@ -33,6 +33,7 @@ _SIGNATURES = {
     "bhSetTuning": (_int, [_int, _int, _int]),
     "bhGetTuning": (None, [_int, C.POINTER(_int), C.POINTER(_int)]),
     "bhSetTileOrder": (_int, [_int]),
+    "bhRenderPipelineNoAlloc": (_int, [_vp, _vp, _P, _vp]),
     "bhMeasureFp32Peak": (C.c_double, []),
     "bhVersion": (C.c_char_p, []),
 }

@@ -215,6 +215,13 @@ cudaError_t pipeline(uchar4* out, float4* accum, float4* bloomA, float4* bloomB,
 
 }  // namespace
 
+TraceParams bh_frame_params(const RenderParams& P, int outMode, void* out)
+{
+    return frameParams(P, outMode, out);
+}
+
+int bh_family_blocks(const RenderParams& P) { return familyBlocks(P); }
+
 extern "C" {
 
 cudaError_t launchRenderPipeline(uchar4* out, float4* accum, float4* bloomA, float4* bloomB,

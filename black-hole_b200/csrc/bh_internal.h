@@ -29,6 +29,12 @@ cudaError_t bh_launch_trace(const TraceParams& P, int precision, bool stats, int
 cudaError_t bh_launch_post(uchar4* out, const float4* accum, float4* hblur, int W, int H,
                            const PostConsts& pc, cudaStream_t stream);
 
+// frame constants of a sanitised view for the given output (bh_api.cpp), and
+// the CTAs per SM the view's metric family is tuned for
+struct RenderParams;
+TraceParams bh_frame_params(const RenderParams& P, int outMode, void* out);
+int bh_family_blocks(const RenderParams& P);
+
 // camera-frame constants of t.camPos / t.M / t.a / t.Q in FP32 and FP64 (bh_camera.cpp)
 void bh_fill_camera_frames(TraceParams& t);
 

@@ -150,6 +150,32 @@ void bhGetTuning(int family, int* refillMin, int* blocksPerSm);
  * outside any stream capture).  Returns 1 when applied, 0 when out of range. */
 int bhSetTileOrder(int mode);
 
+/* ---- allocation-free pipeline (no counterpart in the reference) --------- */
+
+/* Largest half-resolution image ((W+1)/2 * (H+1)/2 pixels) the allocation-free
+ * pipeline accepts with bloom on: 1920x1080 and 2048x1024 fit. */
+#define BH_NOALLOC_MAX_HALF_PIXELS 524288
+
+/* launchRenderPipeline for callers that cannot let a library allocate device
+ * memory -- a frame loop recorded inside CUDA stream capture, where cudaMalloc
+ * is not allowed; a real-time loop that must never stall on the allocator; a
+ * plugin whose host owns all device memory.  The caller still passes the
+ * output (W*H uchar4) and the accumulation buffer (W*H float4, persistent);
+ * the bloom intermediate and the work counter live in one fixed array inside
+ * the library (256 B + BH_NOALLOC_MAX_HALF_PIXELS * 16 B = 8 MiB), which every
+ * GPU that loads libbh.so holds until exit.  The call allocates nothing: it
+ * makes no cudaMalloc or cudaFree and calls no allocating library routine.
+ *  - Frames whose half-resolution image exceeds BH_NOALLOC_MAX_HALF_PIXELS
+ *    are rejected with cudaErrorInvalidValue when bloom is on (nothing is
+ *    launched); with bloom off any size is accepted.
+ *  - The first call on a device looks up the array's device address; make
+ *    that first call before any stream capture begins.
+ *  - All calls on a device share the array and it keeps the last call's
+ *    contents; calls that overlap on the GPU race, so serialise them (one
+ *    stream, or events between streams).
+ *  - Tiles are traced in row-major order; the image is launchRenderPipeline's. */
+cudaError_t bhRenderPipelineNoAlloc(uchar4* out, float4* accum, BH_PARAMS_IN p, cudaStream_t stream);
+
 /* Measured FP32 FMA throughput of the current device, in TFLOP/s, from a
  * dependent-chain FMA kernel timed with CUDA events (blocking). */
 double bhMeasureFp32Peak(void);
