@@ -1,9 +1,9 @@
 """Scene construction: orbit camera, quality presets and the named workloads.
 
 The orbit camera restates the reference application's fillCamera
-(src/main.cpp:186-228) with the body orientation at identity: spin axis +Y,
-camera at (d cos(el) cos(az), d sin(el), d cos(el) sin(az)) looking at the
-origin.  Inclination i maps to elevation 90 deg - i.  Distances are code units
+(src/main.cpp:186-228): spin axis +Y, camera at (d cos(el) cos(az), d sin(el),
+d cos(el) sin(az)) looking at the origin, then the body orientation R = Rz Ry Rx
+(main.cpp:147-166; identity by default).  Inclination i maps to elevation 90 deg - i.  Distances are code units
 with M = 0.5, so "r = 20 rs" is 20.0.
 
 make_params restates the reference test helper makeParams
@@ -21,8 +21,29 @@ from .abi import (BH_KERR, BH_KERR_NEWMAN, BH_REISSNER_NORDSTROM, BH_SCHWARZSCHI
 PRESETS = {"fast": (0.020, 1200), "balanced": (0.012, 2000), "high": (0.007, 3500)}
 
 
-def orbit_camera(P, az, el, dist, fov_deg=60.0):
-    """fillCamera (main.cpp:186-228) for identity body orientation, in float32."""
+def _rotate_body(v, ori):
+    """R = Rz(ori_z) Ry(ori_y) Rx(ori_x) applied to a vector (main.cpp:147-166)."""
+    f32 = np.float32
+    cx, sx = f32(math.cos(ori[0])), f32(math.sin(ori[0]))
+    cy, sy = f32(math.cos(ori[1])), f32(math.sin(ori[1]))
+    cz, sz = f32(math.cos(ori[2])), f32(math.sin(ori[2]))
+    x0, y0, z0 = (f32(t) for t in v)
+    x1, y1, z1 = x0, cx * y0 - sx * z0, sx * y0 + cx * z0
+    x2, y2, z2 = cy * x1 + sy * z1, y1, -sy * x1 + cy * z1
+    return np.array([cz * x2 - sz * y2, sz * x2 + cz * y2, z2], dtype=f32)
+
+
+def _unit(v):
+    f32 = np.float32
+    n = f32(np.sqrt(np.sum(v * v, dtype=f32)))
+    if n < 1e-8:
+        return np.array([0.0, 1.0, 0.0], dtype=f32)
+    return (v / n).astype(f32)
+
+
+def orbit_camera(P, az, el, dist, fov_deg=60.0, ori=(0.0, 0.0, 0.0)):
+    """fillCamera (main.cpp:186-228) in float32: orbit camera looking at the hole,
+    mapped through the body orientation `ori` (Euler X, Y, Z; identity by default)."""
     f32 = np.float32
     ca, sa = f32(math.cos(az)), f32(math.sin(az))
     ce, se = f32(math.cos(el)), f32(math.sin(el))
@@ -35,8 +56,9 @@ def orbit_camera(P, az, el, dist, fov_deg=60.0):
     if rl < 1e-6:
         r, rl = np.array([1.0, 0.0, 0.0], dtype=f32), f32(1.0)
     r = (r / rl).astype(f32)
-    u = np.cross(r, f).astype(f32)
-    u = (u / f32(np.sqrt(np.sum(u * u, dtype=f32)))).astype(f32)
+    p, f, r = (_rotate_body(v, ori) for v in (p, f, r))   # identity for ori = 0
+    f, r = _unit(f), _unit(r)
+    u = _unit(np.cross(r, f).astype(f32))                  # re-orthogonalised up
     P.camPos, P.camForward, P.camRight, P.camUp = p, f, r, u
     P.tanHalfFov = float(f32(math.tan(math.radians(fov_deg) * 0.5)))
     P.aspect = float(f32(P.width) / f32(P.height)) if P.height > 0 else 16.0 / 9.0
@@ -93,11 +115,12 @@ def make_params(derive, model, a_star, q, dPhi=0.012, max_steps=4000, allow_nake
 
 def scene(derive, model, a_star, q, width, height, dist, el_deg, fov_deg, az_deg=0.0,
           preset="balanced", disk=True, hot_spots=True, bloom=True, disk_time=0.0,
-          exposure=1.0):
+          exposure=1.0, ori_deg=(0.0, 0.0, 0.0), allow_naked=False):
     """A rendered frame as the application sets it up (main.cpp:376-478), accumMode 0."""
     P = RenderParams(width=width, height=height)
-    apply_black_hole(P, model, a_star, q, derive)
-    orbit_camera(P, math.radians(az_deg), math.radians(el_deg), dist, fov_deg)
+    apply_black_hole(P, model, a_star, q, derive, allow_naked)
+    orbit_camera(P, math.radians(az_deg), math.radians(el_deg), dist, fov_deg,
+                 tuple(math.radians(o) for o in ori_deg))
     P.dPhi, P.maxSteps = PRESETS[preset]
     P.diskEnabled = 1 if disk else 0
     P.hotSpotsEnabled = 1 if (hot_spots and disk) else 0
