@@ -20,7 +20,7 @@ HERE = os.path.dirname(os.path.abspath(__file__))
 sys.path.insert(0, os.path.dirname(HERE))
 
 from bhrt import lib, scenes  # noqa: E402
-from bhrt.abi import BH_PREC_FP32, BH_PREC_FP64, MODEL_NAMES  # noqa: E402
+from bhrt.abi import BH_PREC_FP32, BH_PREC_FP64, BH_PREC_MIXED, MODEL_NAMES  # noqa: E402
 
 
 def named(name, frame, width, height):
@@ -87,12 +87,12 @@ def main(argv=None):
     ap.add_argument("--no-spots", action="store_true")
     ap.add_argument("--no-bloom", action="store_true")
     ap.add_argument("--naked", action="store_true")
-    ap.add_argument("--fp64", action="store_true")
+    ap.add_argument("--precision", default="fp32", choices=["fp32", "mixed", "fp64"])
     ap.add_argument("--repeat", type=int, default=1)
     ap.add_argument("--out", default=None)
     ap.add_argument("--outdir", default=None)
     a = ap.parse_args(argv)
-    prec = BH_PREC_FP64 if a.fp64 else BH_PREC_FP32
+    prec = {"fp32": BH_PREC_FP32, "mixed": BH_PREC_MIXED, "fp64": BH_PREC_FP64}[a.precision]
 
     if a.cmd == "info":
         P = named(a.scene, a.frame, a.width, a.height) if a.scene else custom(a)
@@ -104,7 +104,7 @@ def main(argv=None):
     if a.cmd == "render":
         P = named(a.scene, a.frame, a.width, a.height) if a.scene else custom(a)
         t = render(P, prec, a.repeat, a.out)
-        print(f"{P.width}x{P.height} {MODEL_NAMES[P.model]}: {min(t):.3f} ms (best of {len(t)})"
+        print(f"{P.width}x{P.height} {MODEL_NAMES[P.model]} {a.precision}: {min(t):.3f} ms (best of {len(t)})"
               + (f" -> {a.out}" if a.out else ""))
         return 0
     # sweep

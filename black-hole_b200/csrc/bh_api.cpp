@@ -185,7 +185,7 @@ int familyBlocks(const RenderParams& P)
 
 cudaError_t trace(TraceParams t, const RenderParams& P, int precision, bool stats, cudaStream_t s)
 {
-    if (precision != BH_PREC_FP32 && precision != BH_PREC_FP64) return cudaErrorInvalidValue;
+    if (precision < BH_PREC_FP32 || precision > BH_PREC_FP64) return cudaErrorInvalidValue;
     if (!t.out) return cudaErrorInvalidValue;
     cudaError_t e = deviceScratch(&t.counter);
     if (e != cudaSuccess) return e;

@@ -30,6 +30,7 @@
 // uses sincos_fast.  The escape direction is rebuilt once per ray with the
 // accurate library sincos.
 // ---------------------------------------------------------------------------
+#include <type_traits>
 #include "bh_shade.cuh"
 #include "bh_internal.h"
 
@@ -112,13 +113,119 @@ BH_DEV void sincos_theta(double x, double& s, double& c) { sincos(x, &s, &c); }
 BH_DEV void sincos_stage(float x, float& s, float& c) { __sincosf(x, &s, &c); }
 BH_DEV void sincos_stage(double x, double& s, double& c) { sincos(x, &s, &c); }
 
+// Cubic Hermite interpolant on a step: value at fraction t of the step of
+// length h, from end values y0, y1 and derivatives d0, d1 (per unit parameter).
+template <class T>
+BH_DEV T hermite(T y0, T y1, T d0, T d1, T h, T t)
+{
+    T t2 = t * t, t3 = t2 * t;
+    return (T(2) * t3 - T(3) * t2 + T(1)) * y0 + (t3 - T(2) * t2 + t) * h * d0 + (T(3) * t2 - T(2) * t3) * y1 +
+           (t3 - t2) * h * d1;
+}
+
+// Root of the Hermite interpolant of f (f0, f1 of opposite sign) by bisection:
+// the equatorial crossing of a step, located to the working precision.
+template <class T>
+BH_DEV T bisect_hermite(T f0, T f1, T d0, T d1, T h)
+{
+    T lo = T(0), hi = T(1);
+    const int iters = sizeof(T) == 8 ? 52 : 24;
+    for (int i = 0; i < iters; ++i)
+    {
+        T mid = T(0.5) * (lo + hi);
+        T fm = hermite(f0, f1, d0, d1, h, mid);
+        if ((fm < T(0)) == (f0 < T(0))) lo = mid; else hi = mid;
+    }
+    return T(0.5) * (lo + hi);
+}
+
+// First equatorial crossing of the ray inside the disk annulus: the
+// "disk-hit" radius and the emitter redshift there, recorded for ray
+// statistics (probe records, surrogate training targets).
+BH_DEV void record_disk_hit(const TraceParams& P, DiskTally& tally, float rHit, float E, float Lz)
+{
+    if (tally.hitR > 0.f || !(rHit >= P.diskInner && rHit <= P.diskOuter)) return;
+    float om = omega_circ(rHit, P.M, P.a, P.Q);
+    tally.hitR = rHit;
+    tally.hitG = (om > 0.f) ? emitter_g(rHit, om, P.M, P.a, P.Q, E, Lz) : 0.f;
+}
+
 // ===========================================================================
 // Spherically symmetric metrics (Schwarzschild, Reissner-Nordstrom)
 // ===========================================================================
-template <class R, bool STATS>
+// One RK4 step of the Binet equation in FP64 from a lower-precision state.
+template <class R>
+BH_DEV void binet_rk4_fp64(R& u, R& du, R h, const CamFrame<double>& F)
+{
+    double U = (double)u, V = (double)du, H = (double)h;
+    const double m3 = 3.0 * F.M, q2 = 2.0 * F.Q2;
+    auto acc = [&](double x) { return (m3 * x - q2 * x * x) * x - x; };
+    const double hh = 0.5 * H;
+    double k1 = acc(U);
+    double u2 = U + hh * V, v2 = V + hh * k1, k2 = acc(u2);
+    double u3 = U + hh * v2, v3 = V + hh * k2, k3 = acc(u3);
+    double u4 = U + H * v3, v4 = V + H * k3, k4 = acc(u4);
+    const double h6 = H / 6.0;
+    U += h6 * (V + 2.0 * v2 + 2.0 * v3 + v4);
+    V += h6 * (k1 + 2.0 * k2 + 2.0 * k3 + k4);
+    u = (R)U;
+    du = (R)V;
+}
+
+// Camera-frame initial data of a spherical-family ray, in precision T.
+template <class T>
+struct SphInit
+{
+    T E, Lz, e2x, e2y, e2z, invB, u, du;
+    bool radial, inward;
+};
+
+template <class T>
+BH_DEV SphInit<T> sph_init(const TraceParams& P, const CamFrame<T>& F, vec3<T> dir)
+{
+    SphInit<T> o;
+    // photon E, Lz (reference src/trace.cuh:213-247 with a = 0)
+    o.E = T(1); o.Lz = T(0);
+    if (!F.camAtOrigin)
+    {
+        T dpc = xdot(F.ephS, dir);
+        T ptUp = xsub(F.rsqS, xdiv(xmul(xmul(dpc, F.AS), F.gtpS), F.gttS));
+        T pfUp = xmul(dpc, F.AS);
+        o.E = -xadd(xmul(F.gttS, ptUp), xmul(F.gtpS, pfUp));
+        o.Lz = xadd(xmul(F.gtpS, ptUp), xmul(F.gppS, pfUp));
+        if (!(o.E > T(1e-6f)) || !finite_p(o.E)) { o.E = T(1); o.Lz = T(0); }
+    }
+    // orbital plane (reference src/trace.cuh:490-521)
+    T ddr = xdot(F.e1, dir);
+    T px = xsub(dir.x, xmul(F.e1[0], ddr));
+    T py = xsub(dir.y, xmul(F.e1[1], ddr));
+    T pz = xsub(dir.z, xmul(F.e1[2], ddr));
+    T pl = xsqrt(xadd(xadd(xmul(px, px), xmul(py, py)), xmul(pz, pz)));
+    o.radial = pl < T(1e-6f);
+    if (o.radial)
+    {   // exactly radial ray (reference src/trace.cuh:447-459, 500-505)
+        const vec3<T> c = widen<T>(tof3(P.camPos));
+        o.inward = xadd(xadd(xmul(dir.x, c.x), xmul(dir.y, c.y)), xmul(dir.z, c.z)) < T(0);
+        return o;
+    }
+    o.inward = false;
+    T ipl = xdiv(T(1), pl);
+    o.e2x = xmul(px, ipl); o.e2y = xmul(py, ipl); o.e2z = xmul(pz, ipl);
+    T bImpact = max_p(xdiv(xmul(F.r0, pl), F.sf0), T(1e-6f));
+    o.invB = T(1) / bImpact;
+    o.u = F.u0;
+    o.du = xdiv(xmul(-F.sf0, ddr), xmul(F.r0, pl));
+    return o;
+}
+
+// MIXED: FP32 state and steps; FP64 initial data, and whole steps in FP64 where
+// the Binet solution turns (|u'| would change sign within the step) or nears
+// the horizon; FP64 location of the equatorial crossing.
+template <class R, bool STATS, bool MIXED = false>
 struct SphRay
 {
     using Real = R;
+    static constexpr bool kKerrFamily = false;
     R u, du, phi, tFlight, invB;
     R e2x, e2y, e2z;                  // in-plane unit vector normal to e1 (e1 is the camera's)
     R ud, dud, phid;                  // state of the last chord direction (deferred)
@@ -132,8 +239,6 @@ struct SphRay
 
     BH_DEV int init(const TraceParams& P, f3 dirf)
     {
-        const CamFrame<R>& F = frame_of<R>(P);
-        const vec3<R> dir = widen<R>(dirf);
         horizon = escaped = haveDir = false;
         accum = v3(0.f, 0.f, 0.f);
         trans = 1.f;
@@ -141,39 +246,27 @@ struct SphRay
         tFlight = R(0);
         prevPos = tof3(P.camPos);
         if (STATS) { tally.samples = 0; tally.hitR = 0.f; tally.hitG = 0.f; I0 = 0.0; }
-
-        // photon E, Lz (reference src/trace.cuh:213-247 with a = 0)
-        R Eph = R(1), Lph = R(0);
-        if (!F.camAtOrigin)
+        bool radial, inward;
+        if constexpr (MIXED)
         {
-            R dpc = xdot(F.ephS, dir);
-            R ptUp = xsub(F.rsqS, xdiv(xmul(xmul(dpc, F.AS), F.gtpS), F.gttS));
-            R pfUp = xmul(dpc, F.AS);
-            Eph = -xadd(xmul(F.gttS, ptUp), xmul(F.gtpS, pfUp));
-            Lph = xadd(xmul(F.gtpS, ptUp), xmul(F.gppS, pfUp));
-            if (!(Eph > R(1e-6f)) || !finite_p(Eph)) { Eph = R(1); Lph = R(0); }
+            SphInit<double> v = sph_init<double>(P, P.cd, widen<double>(dirf));
+            radial = v.radial; inward = v.inward;
+            E = (float)v.E; Lz = (float)v.Lz;
+            e2x = (R)v.e2x; e2y = (R)v.e2y; e2z = (R)v.e2z; invB = (R)v.invB; u = (R)v.u; du = (R)v.du;
         }
-        E = (float)Eph; Lz = (float)Lph;
-
-        // orbital plane (reference src/trace.cuh:490-521)
-        R ddr = xdot(F.e1, dir);
-        R px = xsub(dir.x, xmul(F.e1[0], ddr));
-        R py = xsub(dir.y, xmul(F.e1[1], ddr));
-        R pz = xsub(dir.z, xmul(F.e1[2], ddr));
-        R pl = xsqrt(xadd(xadd(xmul(px, px), xmul(py, py)), xmul(pz, pz)));
-        if (pl < R(1e-6f))
-        {   // exactly radial ray (reference src/trace.cuh:447-459, 500-505)
-            const vec3<R> c = widen<R>(tof3(P.camPos));
-            horizon = xadd(xadd(xmul(dir.x, c.x), xmul(dir.y, c.y)), xmul(dir.z, c.z)) < R(0);
+        else
+        {
+            SphInit<R> v = sph_init<R>(P, frame_of<R>(P), widen<R>(dirf));
+            radial = v.radial; inward = v.inward;
+            E = (float)v.E; Lz = (float)v.Lz;
+            e2x = v.e2x; e2y = v.e2y; e2z = v.e2z; invB = v.invB; u = v.u; du = v.du;
+        }
+        if (radial)
+        {
+            horizon = inward;
             escaped = !horizon;
             return RAY_DONE;
         }
-        R ipl = xdiv(R(1), pl);
-        e2x = xmul(px, ipl); e2y = xmul(py, ipl); e2z = xmul(pz, ipl);
-        R bImpact = max_p(xdiv(xmul(F.r0, pl), F.sf0), R(1e-6f));
-        invB = rcp_p(bImpact);
-        u = F.u0;
-        du = xdiv(xmul(-F.sf0, ddr), xmul(F.r0, pl));
         phi = R(0);
         if (STATS) I0 = binet((R)P.M, (R)P.Q * (R)P.Q, u, du);
         return RAY_LIVE;
@@ -197,19 +290,25 @@ struct SphRay
         R h = min_p(hMax, R(0.10f) * rcp_p(max_p(abs_p(du), R(1e-6f))));
         h = max_p(h, F.hMin);
 
+        const R u0 = u, du0 = du;
         const R m3 = R(3) * M, q2 = R(2) * Q2;
         auto acc = [&](R x) { return (m3 * x - q2 * x * x) * x - x; };
-        R hh = R(0.5f) * h;
-        R k1v = acc(u);
-        R u2 = u + hh * du, v2 = du + hh * k1v;
-        R k2v = acc(u2);
-        R u3 = u + hh * v2, v3_ = du + hh * k2v;
-        R k3v = acc(u3);
-        R u4 = u + h * v3_, v4 = du + h * k3v;
-        R k4v = acc(u4);
-        R h6 = h * R(1.0 / 6.0);
-        u += h6 * (du + R(2) * v2 + R(2) * v3_ + v4);
-        du += h6 * (k1v + R(2) * k2v + R(2) * k3v + k4v);
+        const R k1v = acc(u);
+        if (MIXED && (abs_p(du) < h * abs_p(k1v) || u > R(0.8f) * F.uHor))
+            binet_rk4_fp64(u, du, h, P.cd);      // turning point / horizon approach
+        else
+        {
+            R hh = R(0.5f) * h;
+            R u2 = u + hh * du, v2 = du + hh * k1v;
+            R k2v = acc(u2);
+            R u3 = u + hh * v2, v3_ = du + hh * k2v;
+            R k3v = acc(u3);
+            R u4 = u + h * v3_, v4 = du + h * k3v;
+            R k4v = acc(u4);
+            R h6 = h * R(1.0 / 6.0);
+            u += h6 * (du + R(2) * v2 + R(2) * v3_ + v4);
+            du += h6 * (k1v + R(2) * k2v + R(2) * k3v + k4v);
+        }
         phi += h;
 
         if (!finite_p(u) || !finite_p(du)) { horizon = true; return true; }
@@ -220,6 +319,7 @@ struct SphRay
         ud = u; dud = du; phid = phi; haveDir = true;
         R fR = max_p(R(1) - R(2) * M * u + Q2 * u * u, R(1e-4f));
         tFlight += h * r * r * invB * rcp_p(fR);
+        if (STATS) equator_crossing(P, u0, du0, k1v, h);
 
         if (P.diskOn && trans > 0.01f)
         {
@@ -233,6 +333,26 @@ struct SphRay
         ++step;
         if (u < F.uEscape && du < R(0)) { escaped = true; return true; }
         return false;
+    }
+
+    // Equatorial crossing inside the step (phi - h, phi]: the orbital plane meets
+    // y = 0 at phi* = atan2(-e1y, e2y) + k pi; u(phi*) from the cubic Hermite
+    // interpolant of the step (FP64 in MIXED and FP64 modes).
+    BH_DEV void equator_crossing(const TraceParams& P, R u0, R du0, R ddu0, R h)
+    {
+        using T = typename std::conditional<MIXED, double, R>::type;
+        const CamFrame<T>& F = frame_of<T>(P);
+        const T e1y = F.e1[1], e2 = (T)e2y;
+        if (abs_p(e1y) + abs_p(e2) < T(1e-12)) return;   // orbit in the equatorial plane
+        const T pc = atan2(-e1y, e2), pi = T(3.14159265358979323846);
+        const T p0 = (T)phi - (T)h;
+        T k = ceil((p0 - pc) / pi);
+        T ps = pc + k * pi;
+        if (ps <= p0) ps += pi;
+        if (ps > (T)phi) return;
+        const T uh = hermite((T)u0, (T)u, (T)du0, (T)du, (T)h, (ps - p0) / (T)h);
+        (void)ddu0;
+        if (uh > T(0)) record_disk_hit(P, tally, (float)(T(1) / uh), E, Lz);
     }
 
     BH_DEV void exhaust(const TraceParams& P)
@@ -334,10 +454,46 @@ BH_DEV KerrEval<R> kerr_rhs(const CamFrame<R>& F, const KerrConsts<R>& k, R r, R
     return o;
 }
 
-template <class R, bool STATS>
+// One RK4 step of the Kerr-Newman system in FP64 from an FP32 state (the
+// right-hand side at the start is re-evaluated in FP64).  Out of line so the
+// FP32 step loop keeps its register budget.
+struct KerrStep64 { float r, th, ph, pr, pth, dr4, dth4, dph4; };
+
+static __device__ __noinline__ KerrStep64 kerr_rk4_fp64(const CamFrame<double>& F, float Ef, float Lzf, float r0,
+                                                        float th0, float ph0, float pr0, float pth0, float hf)
+{
+    const double E = Ef, Lz = Lzf, h = hf;
+    const KerrConsts<double> k{E, Lz, F.a * E, E * F.a2 - F.a * Lz, 2.0 * E};
+    double r = r0, th = th0, ph = ph0, pr = pr0, pth = pth0, s, c;
+    sincos(th, &s, &c);
+    KerrDeriv<double> d1 = kerr_rhs(F, k, r, s, c, pr, pth).d;
+    const double hh = 0.5 * h;
+    sincos(th + hh * d1.th, &s, &c);
+    KerrDeriv<double> d2 = kerr_rhs(F, k, r + hh * d1.r, s, c, pr + hh * d1.pr, pth + hh * d1.pth).d;
+    sincos(th + hh * d2.th, &s, &c);
+    KerrDeriv<double> d3 = kerr_rhs(F, k, r + hh * d2.r, s, c, pr + hh * d2.pr, pth + hh * d2.pth).d;
+    sincos(th + h * d3.th, &s, &c);
+    KerrDeriv<double> d4 = kerr_rhs(F, k, r + h * d3.r, s, c, pr + h * d3.pr, pth + h * d3.pth).d;
+    const double h6 = h / 6.0;
+    KerrStep64 o;
+    o.r = (float)(r + h6 * (d1.r + 2.0 * d2.r + 2.0 * d3.r + d4.r));
+    o.th = (float)(th + h6 * (d1.th + 2.0 * d2.th + 2.0 * d3.th + d4.th));
+    o.ph = (float)(ph + h6 * (d1.ph + 2.0 * d2.ph + 2.0 * d3.ph + d4.ph));
+    o.pr = (float)(pr + h6 * (d1.pr + 2.0 * d2.pr + 2.0 * d3.pr + d4.pr));
+    o.pth = (float)(pth + h6 * (d1.pth + 2.0 * d2.pth + 2.0 * d3.pth + d4.pth));
+    o.dr4 = (float)d4.r; o.dth4 = (float)d4.th; o.dph4 = (float)d4.ph;
+    return o;
+}
+
+// MIXED: FP32 state and steps; FP64 tetrad initial data, whole steps in FP64
+// at radial turning points (p_r would change sign within the step) and on
+// horizon approach (r < 1.5 r_floor), and FP64 bisection of the equatorial
+// crossing.
+template <class R, bool STATS, bool MIXED = false>
 struct KerrRay
 {
     using Real = R;
+    static constexpr bool kKerrFamily = true;
     R r, th, ph, pr, pth;   // Boyer-Lindquist state
     R s, c;                 // sin/cos of th
     KerrConsts<R> k;        // E, Lz and their products
@@ -362,16 +518,32 @@ struct KerrRay
     BH_DEV int init(const TraceParams& P, f3 dirf)
     {   // reference src/trace.cuh:703-739: the per-ray remainder of the tetrad map
         const CamFrame<R>& F = frame_of<R>(P);
-        const vec3<R> dir = widen<R>(dirf);
-        R drc = xdot(F.er, dir), dtc = xdot(F.eth, dir), dpc = xdot(F.eph, dir);
-        R ptUp = xsub(F.rsq, xdiv(xmul(xmul(dpc, F.A), F.gtp), F.gtt));
-        R pfUp = xmul(dpc, F.A);
-        const R E = -xadd(xmul(F.gtt, ptUp), xmul(F.gtp, pfUp));
-        const R Lz = xadd(xmul(F.gtp, ptUp), xmul(F.gpp, pfUp));
+        R E, Lz;
+        if constexpr (MIXED)
+        {   // FP64 tetrad map, each result rounded once
+            const CamFrame<double>& D = P.cd;
+            const vec3<double> dir = widen<double>(dirf);
+            double drc = xdot(D.er, dir), dtc = xdot(D.eth, dir), dpc = xdot(D.eph, dir);
+            double ptUp = xsub(D.rsq, xdiv(xmul(xmul(dpc, D.A), D.gtp), D.gtt));
+            double pfUp = xmul(dpc, D.A);
+            E = (R)(-xadd(xmul(D.gtt, ptUp), xmul(D.gtp, pfUp)));
+            Lz = (R)xadd(xmul(D.gtp, ptUp), xmul(D.gpp, pfUp));
+            pr = (R)xmul(drc, D.sqSD);
+            pth = (R)xmul(dtc, D.sqS);
+        }
+        else
+        {
+            const vec3<R> dir = widen<R>(dirf);
+            R drc = xdot(F.er, dir), dtc = xdot(F.eth, dir), dpc = xdot(F.eph, dir);
+            R ptUp = xsub(F.rsq, xdiv(xmul(xmul(dpc, F.A), F.gtp), F.gtt));
+            R pfUp = xmul(dpc, F.A);
+            E = -xadd(xmul(F.gtt, ptUp), xmul(F.gtp, pfUp));
+            Lz = xadd(xmul(F.gtp, ptUp), xmul(F.gpp, pfUp));
+            pr = xmul(drc, F.sqSD);
+            pth = xmul(dtc, F.sqS);
+        }
         k.E = E; k.Lz = Lz; k.aE = F.a * E; k.c1 = E * F.a2 - F.a * Lz; k.twoE = R(2) * E;
         r = F.r0; th = F.th0; ph = F.ph0;
-        pr = xmul(drc, F.sqSD);
-        pth = xmul(dtc, F.sqS);
         sincos_theta(th, s, c);
         KerrEval<R> ev = kerr_rhs(F, k, r, s, c, pr, pth);
         d1 = ev.d;
@@ -431,6 +603,19 @@ struct KerrRay
             capLen = max_p(R(1.2f), R(0.22f) * r);
         h = min_p(h, capLen * rcp_p(spd));
 
+        const R rS = r, thS = th, drS = d1.r, dthS = d1.th;    // step start (crossing search)
+        R dl0 = R(0), dl1 = R(0), dl2 = R(0);                 // the final stage's derivative
+        if constexpr (MIXED)
+        {
+            if (abs_p(pr) < h * abs_p(d1.pr) || r < F.rFloor * R(1.5f))
+            {
+                KerrStep64 o = kerr_rk4_fp64(P.cd, k.E, k.Lz, r, th, ph, pr, pth, h);
+                r = o.r; th = o.th; ph = o.ph; pr = o.pr; pth = o.pth;
+                dl0 = o.dr4; dl1 = o.dth4; dl2 = o.dph4;
+                return finish_step(P, F, h, rS, thS, drS, dthS, dl0, dl1, dl2);
+            }
+        }
+
         // classic RK4
         const R hh = R(0.5f) * h;
         R sx, cx;
@@ -453,7 +638,14 @@ struct KerrRay
         ph += h6 * (sph + d4.ph);
         pr += h6 * (spr + d4.pr);
         pth += h6 * (spth + d4.pth);
+        return finish_step(P, F, h, rS, thS, drS, dthS, d4.r, d4.th, d4.ph);
+    }
 
+    // Rest of a loop iteration after the RK4 update: pole guard, the next
+    // step's first right-hand side with the slow-light term, disk chord.
+    BH_DEV bool finish_step(const TraceParams& P, const CamFrame<R>& F, R h, R rS, R thS, R drS, R dthS,
+                            R d4r, R d4th, R d4ph)
+    {
         // pole reflection guard
         if (th < R(1e-3f)) { th = R(1e-3f); pth = abs_p(pth); }
         else if (th > R(kPiF - 1e-3f)) { th = R(kPiF - 1e-3f); pth = -abs_p(pth); }
@@ -461,7 +653,7 @@ struct KerrRay
         if (step == P.maxSteps)
         {
             R* dl = last_deriv();
-            dl[0] = d4.r; dl[1] = d4.th; dl[2] = d4.ph;
+            dl[0] = d4r; dl[1] = d4th; dl[2] = d4ph;
         }
 
         // next step's first right-hand side; its Sigma, Delta, P give the slow
@@ -475,6 +667,7 @@ struct KerrRay
             const R dtdl = (F.a * (k.Lz - k.aE * sc * sc) + (r * r + F.a2) * ev.Pp * ev.iDelT) * ev.iS;
             tFlight += h * abs_p(dtdl);
         }
+        if (STATS) equator_crossing(P, h, rS, thS, drS, dthS);
         if (P.diskOn)
         {
             R sp, cp;
@@ -486,6 +679,19 @@ struct KerrRay
             prevPos = pos;
         }
         return false;
+    }
+
+    // Equatorial crossing inside the last step: bisection of the cubic Hermite
+    // interpolant of theta over the step (FP64 in MIXED and FP64 modes), r there.
+    BH_DEV void equator_crossing(const TraceParams& P, R h, R rS, R thS, R drS, R dthS)
+    {
+        using T = typename std::conditional<MIXED, double, R>::type;
+        const T half = T(1.57079632679489661923);
+        const T f0 = (T)thS - half, f1 = (T)th - half;
+        if (!((f0 < T(0)) != (f1 < T(0)))) return;
+        const T t = bisect_hermite(f0, f1, (T)dthS, (T)d1.th, (T)h);
+        const T rh = hermite((T)rS, (T)r, (T)drS, (T)d1.r, (T)h, t);
+        record_disk_hit(P, tally, (float)rh, (float)k.E, (float)k.Lz);
     }
 
     BH_DEV void exhaust(const TraceParams& P)

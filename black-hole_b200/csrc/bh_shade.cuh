@@ -125,7 +125,9 @@ BH_DEV float wrap_pi(float d)
     return d - kPiF;
 }
 
-// Per-ray disk bookkeeping kept only when the caller asks for ray statistics.
+// Per-ray disk bookkeeping kept only when the caller asks for ray statistics:
+// contributing sub-samples, and the radius / emitter redshift of the first
+// equatorial crossing inside the disk annulus (the "disk hit").
 struct DiskTally
 {
     int samples;
@@ -229,13 +231,8 @@ BH_DEV void disk_segment(const TraceParams& P, float E, float Lz, f3 a, f3 b, fl
         if (spotBoost > 1e-4f) k += spotBoost * g3 * P.emisK * 0.55f * ((0.12f + dens) * ds);
         accum = accum + col * (k * trans);
 
-        float before = trans;
         trans *= __expf(-(P.absK * w * (1.f + 0.35f * dens)));
-        if (STATS)
-        {
-            tally.samples++;
-            if (before >= 0.5f && trans < 0.5f) { tally.hitR = rc; tally.hitG = g; }
-        }
+        if (STATS) tally.samples++;
         if (trans < 0.012f) return;
     }
 }

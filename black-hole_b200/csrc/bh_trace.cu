@@ -121,12 +121,15 @@ BH_DEV void shade_slot(const TraceParams& P, const PackedRay<typename Ray::Real>
     }
 }
 
-// register budget: FP32 render kernels BH_TRACE_MIN_BLOCKS CTAs per SM; the
-// FP64 oracle and the statistics (probe) kernels carry more state, 4 CTAs
+// Register budget (CTAs of 128 threads resident per SM): the spherical FP32
+// render kernel fits 72 registers (7 CTAs); the Kerr-Newman FP32 kernels need
+// 80 (6 CTAs) to stay spill-free in the step loop; FP64 and statistics (probe)
+// kernels carry more state (4 CTAs).  The runtime may run fewer (bhSetTuning).
 template <class Ray, bool STATS>
 constexpr int min_blocks()
 {
-    return (sizeof(typename Ray::Real) == 4 && !STATS) ? BH_TRACE_MIN_BLOCKS : 4;
+    if (sizeof(typename Ray::Real) != 4 || STATS) return 4;
+    return Ray::kKerrFamily ? 6 : BH_TRACE_MIN_BLOCKS;
 }
 
 template <class Ray, bool STATS>
@@ -266,6 +269,13 @@ cudaError_t bh_launch_trace(const TraceParams& P, int precision, bool stats, int
     if (P.nRays == 0) return cudaSuccess;
     const bool kerr = (P.model == 2 || P.model == 3);
     const bool dbl = (precision == BH_PREC_FP64);
+    if (precision == BH_PREC_MIXED)
+    {
+        if (kerr) return stats ? launch_one<KerrRay<float, true, true>, true>(P, blocksPerSm, stream)
+                               : launch_one<KerrRay<float, false, true>, false>(P, blocksPerSm, stream);
+        return stats ? launch_one<SphRay<float, true, true>, true>(P, blocksPerSm, stream)
+                     : launch_one<SphRay<float, false, true>, false>(P, blocksPerSm, stream);
+    }
     if (kerr)
     {
         if (dbl) return stats ? launch_one<KerrRay<double, true>, true>(P, blocksPerSm, stream)

@@ -489,9 +489,44 @@ struct DiskPhoton { float E, Lz, a, Q; };            /* trace.cuh:203-209 */
 
 struct DiskTally                                     /* additions: not in the reference */
 {
-    int samples = 0;
-    float hitR = 0.f, hitG = 0.f;
+    int samples = 0;             /* contributing disk sub-samples */
+    float hitR = 0.f, hitG = 0.f; /* first equatorial crossing inside the disk annulus, g there */
 };
+
+/* Cubic Hermite interpolant over a step of length h at fraction t. */
+inline double hermite(double y0, double y1, double d0, double d1, double h, double t)
+{
+    double t2 = t * t, t3 = t2 * t;
+    return (2 * t3 - 3 * t2 + 1) * y0 + (t3 - 2 * t2 + t) * h * d0 + (3 * t2 - 2 * t3) * y1 + (t3 - t2) * h * d1;
+}
+
+/* Disk hit (addition): record the first equatorial crossing whose radius lies
+ * in [diskInner, diskOuter], with the emitter redshift of the ray there. */
+inline void recordHit(const RenderParams& P, DiskTally& t, double r, float E, float Lz)
+{
+    if (t.hitR > 0.f || !(r >= P.diskInner && r <= P.diskOuter)) return;
+    float rf = (float)r;
+    t.hitR = rf;
+    t.hitG = emitterG(rf, P.M, P.aSpin, P.Qc, E, Lz);
+}
+
+/* Kerr-Newman: theta crosses pi/2 within the step -> bisection of the Hermite
+ * interpolant of theta, r there (FP64). */
+inline void kerrCrossing(const RenderParams& P, DiskTally& t, double r0, double th0, double dr0, double dth0,
+                         double r1, double th1, double dr1, double dth1, double h, float E, float Lz)
+{
+    const double half = 1.57079632679489661923;
+    const double f0 = th0 - half, f1 = th1 - half;
+    if (!((f0 < 0.0) != (f1 < 0.0))) return;
+    double lo = 0.0, hi = 1.0;
+    for (int i = 0; i < 52; ++i)
+    {
+        double mid = 0.5 * (lo + hi);
+        double fm = hermite(f0, f1, dth0, dth1, h, mid);
+        if ((fm < 0.0) == (f0 < 0.0)) lo = mid; else hi = mid;
+    }
+    recordHit(P, t, hermite(r0, r1, dr0, dr1, h, 0.5 * (lo + hi)), E, Lz);
+}
 
 inline float wrapPi(float d)                         /* trace.cuh:250-255 */
 {
@@ -602,10 +637,8 @@ void diskSegment(const RenderParams& P, const DiskPhoton& ph, F3 a, F3 b, float 
         accum = accum + add * trans;
 
         float tau = absK * w * (1.f + 0.35f * dens);
-        float before = trans;
         trans *= expf(-tau);
         tally.samples++;
-        if (before >= 0.5f && trans < 0.5f) { tally.hitR = rc; tally.hitG = g; }
         if (trans < 0.012f) return;
     }
 }
@@ -655,7 +688,7 @@ void conservedEL(V3<T> o, V3<T> dir, T M, T a, T Q, T& E, T& Lz)   /* trace.cuh:
 }
 
 template <class T>
-Ray traceSpherical(const RenderParams& P, V3<T> origin, V3<T> dir)   /* trace.cuh:466-611 */
+Ray traceSpherical(const RenderParams& P, V3<T> origin, V3<T> dir, bool wantStats)   /* trace.cuh:466-611 */
 {
     Ray R;
     R.escDir = tof(dir);
@@ -709,6 +742,7 @@ Ray traceSpherical(const RenderParams& P, V3<T> origin, V3<T> dir)   /* trace.cu
         h = Fmin(hMax, T(0.10f) / Fmax(Fabs(du), T(1e-6f)));
         if (h < dPhi * T(0.03f)) h = dPhi * T(0.03f);
 
+        const T uS = u, duS = du;
         T k1u = du;
         T k1v = acc(u);
         T u2 = u + T(0.5f) * h * k1u;
@@ -741,6 +775,22 @@ Ray traceSpherical(const RenderParams& P, V3<T> origin, V3<T> dir)   /* trace.cu
 
         T fR = Fmax(sphF(r, M, Qc), T(1e-4f));
         tFlight += h * (r * r) / (bImpact * fR);
+        if (wantStats)
+        {   /* disk hit (addition): the plane crosses y = 0 at phi* = atan2(-e1y, e2y) + k pi */
+            const double e1y = (double)e1.y, e2y = (double)e2.y;
+            if (std::fabs(e1y) + std::fabs(e2y) >= 1e-12)
+            {
+                const double pc = std::atan2(-e1y, e2y), pi = 3.14159265358979323846;
+                const double p0 = (double)phi - (double)h;
+                double ps = pc + std::ceil((p0 - pc) / pi) * pi;
+                if (ps <= p0) ps += pi;
+                if (ps <= (double)phi)
+                {
+                    double uh = hermite(uS, u, duS, du, h, (ps - p0) / (double)h);
+                    if (uh > 0.0) recordHit(P, R.tally, 1.0 / uh, ctx.E, ctx.Lz);
+                }
+            }
+        }
 
         if (P.diskEnabled && R.trans > 0.01f)
             diskSegment(P, ctx, tof(prevPos), tof(pos), (float)((T)P.diskTime - tFlight),
@@ -876,10 +926,14 @@ Ray traceKerr(const RenderParams& P, V3<T> origin, V3<T> dir, bool wantStats)   
     bool haveDeriv = false;
     int step = 0;
 
+    /* disk hit bookkeeping (addition): start of the previous step */
+    double cR = 0, cTh = 0, cDr = 0, cDth = 0, cH = 0;
     for (; step < P.maxSteps; ++step)
     {
         T Kv;
         KS<T> d1 = kerrRHS(M, a, Q, E, Lz, y, Kv);
+        if (wantStats && step > 0)
+            kerrCrossing(P, R.tally, cR, cTh, cDr, cDth, y.r, y.th, d1.r, d1.th, cH, ctx.E, ctx.Lz);
         if (!Finite(y.r) || !Finite(y.pr) || !Finite(y.pth) || !Finite(d1.r) || !Finite(d1.pr))
         { R.horizon = true; break; }
         if (y.r <= rCap * T(1.002f) + T(1e-3f)) { R.horizon = true; break; }
@@ -911,6 +965,7 @@ Ray traceKerr(const RenderParams& P, V3<T> origin, V3<T> dir, bool wantStats)   
         else capLen = Fmax(T(1.2f), T(0.22f) * y.r);
         h = Fmin(h, capLen / spd);
 
+        cR = y.r; cTh = y.th; cDr = d1.r; cDth = d1.th; cH = h;
         T kv2, kv3, kv4;
         KS<T> y2 = {y.r + T(0.5f) * h * d1.r, y.th + T(0.5f) * h * d1.th,
                     y.ph + T(0.5f) * h * d1.ph, y.pr + T(0.5f) * h * d1.pr,
@@ -961,6 +1016,12 @@ Ray traceKerr(const RenderParams& P, V3<T> origin, V3<T> dir, bool wantStats)   
         }
     }
     R.steps = step;
+    if (wantStats && step >= P.maxSteps && step > 0)
+    {   /* budget spent: the last step's crossing */
+        T Kv;
+        KS<T> dEnd = kerrRHS(M, a, Q, E, Lz, y, Kv);
+        kerrCrossing(P, R.tally, cR, cTh, cDr, cDth, y.r, y.th, dEnd.r, dEnd.th, cH, ctx.E, ctx.Lz);
+    }
     if (!R.horizon && !R.escaped)
     {
         if (y.r < T(6) * M) R.horizon = true;
@@ -988,7 +1049,7 @@ Ray traceRay(const RenderParams& P, F3 origin, F3 dir, bool wantStats)   /* trac
 {
     if (P.model == BH_KERR || P.model == BH_KERR_NEWMAN)
         return traceKerr<T>(P, cvt<T>(origin), cvt<T>(dir), wantStats);
-    return traceSpherical<T>(P, cvt<T>(origin), cvt<T>(dir));
+    return traceSpherical<T>(P, cvt<T>(origin), cvt<T>(dir), wantStats);
 }
 
 Ray traceAny(const RenderParams& P, F3 origin, F3 dir, bool wantStats, int precision)
