@@ -83,6 +83,15 @@ assert RenderParams.camPos.offset == 12 and RenderParams.dPhi.offset == 100
 assert RenderParams.bloomStrength.offset == 156
 
 
+class BHView(C.Structure):
+    """One view of a batch (include/bh_launch.h): parameters + device buffers."""
+    _fields_ = [("params", RenderParams), ("out", C.c_void_p), ("accum", C.c_void_p),
+                ("bloomA", C.c_void_p), ("bloomB", C.c_void_p)]
+
+
+assert C.sizeof(BHView) == 160 + 4 * 8
+
+
 class BHDerived(C.Structure):
     _fields_ = [("a", C.c_float), ("Q", C.c_float), ("rPlus", C.c_float), ("rMinus", C.c_float),
                 ("rPhoton", C.c_float), ("rErgo", C.c_float), ("rIsco", C.c_float),

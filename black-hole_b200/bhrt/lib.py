@@ -33,6 +33,13 @@ _SIGNATURES = {
     "bhSetTuning": (_int, [_int, _int, _int]),
     "bhGetTuning": (None, [_int, C.POINTER(_int), C.POINTER(_int)]),
     "bhSetTileOrder": (_int, [_int]),
+    "bhGetTileOrder": (_int, []),
+    "bhRenderBatch": (_int, [_vp, _int, _vp]),
+    "bhBatchGraphCreate": (_int, [C.POINTER(_vp), _vp, _int]),
+    "bhBatchGraphUpdate": (_int, [_vp, _vp, _int]),
+    "bhBatchGraphLaunch": (_int, [_vp, _vp]),
+    "bhBatchGraphDestroy": (None, [_vp]),
+    "bhAutotune": (_int, [_P, C.POINTER(_int), C.POINTER(_int), C.POINTER(_int), C.POINTER(C.c_float)]),
     "bhRenderPipelineNoAlloc": (_int, [_vp, _vp, _P, _vp]),
     "bhMeasureFp32Peak": (C.c_double, []),
     "bhVersion": (C.c_char_p, []),

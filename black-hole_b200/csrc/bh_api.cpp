@@ -222,6 +222,8 @@ TraceParams bh_frame_params(const RenderParams& P, int outMode, void* out)
 
 int bh_family_blocks(const RenderParams& P) { return familyBlocks(P); }
 
+cudaError_t bh_device_counter(unsigned** out) { return deviceScratch(out); }
+
 extern "C" {
 
 cudaError_t launchRenderPipeline(uchar4* out, float4* accum, float4* bloomA, float4* bloomB,
@@ -307,6 +309,8 @@ int bhSetTileOrder(int mode)
     gTileOrderMode = mode;
     return 1;
 }
+
+int bhGetTileOrder(void) { return gTileOrderMode; }
 
 void bhGetTuning(int family, int* refillMin, int* blocksPerSm)
 {

@@ -1,0 +1,335 @@
+// ---------------------------------------------------------------------------
+// bh_batch.cpp -- many views in one persistent launch, its CUDA-graph form,
+// and the autotuner of the tracing kernels' work distribution.
+//
+// No counterpart in the reference, which renders one view per call
+// (src/black_hole_kernel.cu:108-134).  A batch is equivalent to calling
+// launchRenderPipeline for every view in turn: same sanitising, same images.
+// What changes is scheduling: every view's 8x4-pixel tiles go into one device
+// work queue, traced by one persistent kernel (bh_trace.cu, batch_kernel), so
+// small views, large views and both metric families share the GPU with no
+// per-view launch gaps or tails.  Views are queued in order of estimated cost
+// (pixels x family factor), longest first, so the batch ends on cheap tiles.
+// ---------------------------------------------------------------------------
+#include <algorithm>
+#include <mutex>
+#include <vector>
+#include <cuda_runtime.h>
+#include "bh_launch.h"
+#include "bh_internal.h"
+
+namespace {
+
+bool isKerrModel(int m) { return m == BH_KERR || m == BH_KERR_NEWMAN; }
+
+struct Plan
+{
+    std::vector<int> order;               // trace position -> view index
+    std::vector<RenderParams> params;     // sanitised, by view index
+    std::vector<TraceParams> table;       // trace order
+    std::vector<unsigned> base;           // n + 1 tile prefix sums, trace order
+};
+
+cudaError_t checkView(const BHView& v, const RenderParams& P)
+{
+    if (!v.out || !v.accum) return cudaErrorInvalidValue;
+    if (P.bloomEnabled && !v.bloomB) return cudaErrorInvalidValue;
+    return cudaSuccess;
+}
+
+// Sanitise every view and lay out the work queue.  With `keepOrder` the trace
+// order of a previous plan is reused (graph updates keep their layout).
+cudaError_t makePlan(const BHView* views, int n, Plan& pl, bool keepOrder)
+{
+    if (n < 0 || (n > 0 && !views)) return cudaErrorInvalidValue;
+    pl.params.resize(n);
+    for (int i = 0; i < n; ++i)
+    {
+        pl.params[i] = views[i].params;
+        bhSanitizeRenderParams(&pl.params[i]);
+        cudaError_t e = checkView(views[i], pl.params[i]);
+        if (e != cudaSuccess) return e;
+    }
+    if (!keepOrder)
+    {
+        pl.order.resize(n);
+        for (int i = 0; i < n; ++i) pl.order[i] = i;
+        auto cost = [&](int i) {
+            const RenderParams& P = pl.params[i];
+            return (double)P.width * P.height * (isKerrModel(P.model) ? 3.0 : 1.0);
+        };
+        std::stable_sort(pl.order.begin(), pl.order.end(), [&](int a, int b) { return cost(a) > cost(b); });
+    }
+    pl.table.resize(n);
+    pl.base.assign(n + 1, 0u);
+    for (int k = 0; k < n; ++k)
+    {
+        const int i = pl.order[k];
+        TraceParams t = bh_frame_params(pl.params[i], BH_OUT_ACCUM, views[i].accum);
+        t.tileOrder = nullptr;
+        t.counter = nullptr;
+        pl.table[k] = t;
+        const unsigned tiles = (unsigned)t.tilesX * (unsigned)((t.H + 3) / 4);
+        pl.base[k + 1] = pl.base[k] + tiles;
+    }
+    return cudaSuccess;
+}
+
+cudaError_t launchPlan(const Plan& pl, const BHView* views, const TraceParams* dTable, const unsigned* dBase,
+                       unsigned* counter, cudaStream_t s)
+{
+    const int n = (int)pl.table.size();
+    int blocks = 0;
+    bhGetTuning(1, nullptr, &blocks);
+    cudaError_t e = bh_launch_batch(dTable, dBase, n, pl.base[n], counter, blocks, s);
+    if (e != cudaSuccess) return e;
+    for (int i = 0; i < n; ++i)
+    {
+        const RenderParams& P = pl.params[i];
+        PostConsts pc{P.exposure, P.bloomStrength, P.bloomEnabled ? 1 : 0, P.swapRB};
+        e = bh_launch_post(views[i].out, views[i].accum, views[i].bloomB, P.width, P.height, pc, s);
+        if (e != cudaSuccess) return e;
+    }
+    return cudaSuccess;
+}
+
+// per-device tables of the immediate-mode batch (grown on demand)
+constexpr int kMaxDevices = 64;
+struct DevTables
+{
+    TraceParams* table = nullptr;
+    unsigned* base = nullptr;
+    size_t cap = 0;
+};
+std::mutex gLock;
+DevTables gTables[kMaxDevices];
+
+cudaError_t ensureTables(int n, DevTables** out)
+{
+    int dev = 0;
+    cudaError_t e = cudaGetDevice(&dev);
+    if (e != cudaSuccess) return e;
+    if (dev < 0 || dev >= kMaxDevices) return cudaErrorInvalidDevice;
+    DevTables& t = gTables[dev];
+    if (t.cap < (size_t)n)
+    {
+        if (t.table) cudaFree(t.table);
+        if (t.base) cudaFree(t.base);
+        t.table = nullptr;
+        t.base = nullptr;
+        t.cap = 0;
+        size_t cap = std::max<size_t>(64, (size_t)n);
+        if ((e = cudaMalloc(&t.table, cap * sizeof(TraceParams))) != cudaSuccess) return e;
+        if ((e = cudaMalloc(&t.base, (cap + 1) * sizeof(unsigned))) != cudaSuccess) return e;
+        t.cap = cap;
+    }
+    *out = &t;
+    return cudaSuccess;
+}
+
+}  // namespace
+
+// ---------------------------------------------------------------------------
+// immediate mode
+// ---------------------------------------------------------------------------
+extern "C" cudaError_t bhRenderBatch(const BHView* views, int n, cudaStream_t stream)
+{
+    Plan pl;
+    cudaError_t e = makePlan(views, n, pl, false);
+    if (e != cudaSuccess || n == 0) return e;
+    std::lock_guard<std::mutex> g(gLock);
+    DevTables* t = nullptr;
+    if ((e = ensureTables(n, &t)) != cudaSuccess) return e;
+    unsigned* counter = nullptr;
+    if ((e = bh_device_counter(&counter)) != cudaSuccess) return e;
+    // pageable sources: the copies are staged before the calls return
+    if ((e = cudaMemcpyAsync(t->table, pl.table.data(), n * sizeof(TraceParams), cudaMemcpyHostToDevice, stream)))
+        return e;
+    if ((e = cudaMemcpyAsync(t->base, pl.base.data(), (n + 1) * sizeof(unsigned), cudaMemcpyHostToDevice, stream)))
+        return e;
+    return launchPlan(pl, views, t->table, t->base, counter, stream);
+}
+
+// ---------------------------------------------------------------------------
+// CUDA-graph mode
+// ---------------------------------------------------------------------------
+struct BHBatchGraph
+{
+    int device = 0, n = 0;
+    std::vector<BHView> views;
+    Plan plan;
+    TraceParams* dTable = nullptr;
+    unsigned* dBase = nullptr;
+    unsigned* dCounter = nullptr;
+    unsigned char* hPinned = nullptr;     // table + base, the graph's copy source
+    cudaGraph_t graph = nullptr;
+    cudaGraphExec_t exec = nullptr;
+    cudaEvent_t done = nullptr;
+};
+
+namespace {
+
+void stage(BHBatchGraph& G)
+{
+    const size_t tb = G.n * sizeof(TraceParams);
+    std::copy(reinterpret_cast<const unsigned char*>(G.plan.table.data()),
+              reinterpret_cast<const unsigned char*>(G.plan.table.data()) + tb, G.hPinned);
+    std::copy(reinterpret_cast<const unsigned char*>(G.plan.base.data()),
+              reinterpret_cast<const unsigned char*>(G.plan.base.data()) + (G.n + 1) * sizeof(unsigned),
+              G.hPinned + tb);
+}
+
+void release(BHBatchGraph* G)
+{
+    if (!G) return;
+    if (G->exec) cudaGraphExecDestroy(G->exec);
+    if (G->graph) cudaGraphDestroy(G->graph);
+    if (G->done) cudaEventDestroy(G->done);
+    if (G->dTable) cudaFree(G->dTable);
+    if (G->dBase) cudaFree(G->dBase);
+    if (G->dCounter) cudaFree(G->dCounter);
+    if (G->hPinned) cudaFreeHost(G->hPinned);
+    delete G;
+}
+
+}  // namespace
+
+extern "C" cudaError_t bhBatchGraphCreate(BHBatchGraph** out, const BHView* views, int n)
+{
+    if (!out || n <= 0 || !views) return cudaErrorInvalidValue;
+    *out = nullptr;
+    BHBatchGraph* G = new BHBatchGraph();
+    G->n = n;
+    G->views.assign(views, views + n);
+    cudaError_t e = makePlan(views, n, G->plan, false);
+    cudaStream_t s = nullptr;
+    const size_t tb = n * sizeof(TraceParams), bb = (n + 1) * sizeof(unsigned);
+    if (e == cudaSuccess) e = cudaGetDevice(&G->device);
+    if (e == cudaSuccess) e = cudaMalloc(&G->dTable, tb);
+    if (e == cudaSuccess) e = cudaMalloc(&G->dBase, bb);
+    if (e == cudaSuccess) e = cudaMalloc(&G->dCounter, 256);
+    if (e == cudaSuccess) e = cudaMallocHost(&G->hPinned, tb + bb);
+    if (e == cudaSuccess) e = cudaEventCreateWithFlags(&G->done, cudaEventDisableTiming);
+    if (e == cudaSuccess) e = cudaStreamCreateWithFlags(&s, cudaStreamNonBlocking);
+    if (e != cudaSuccess) { release(G); if (s) cudaStreamDestroy(s); return e; }
+    stage(*G);
+    e = cudaStreamBeginCapture(s, cudaStreamCaptureModeThreadLocal);
+    if (e == cudaSuccess)
+    {
+        cudaError_t le = cudaMemcpyAsync(G->dTable, G->hPinned, tb, cudaMemcpyHostToDevice, s);
+        if (le == cudaSuccess) le = cudaMemcpyAsync(G->dBase, G->hPinned + tb, bb, cudaMemcpyHostToDevice, s);
+        if (le == cudaSuccess) le = launchPlan(G->plan, views, G->dTable, G->dBase, G->dCounter, s);
+        e = cudaStreamEndCapture(s, &G->graph);
+        if (le != cudaSuccess) e = le;
+    }
+    if (e == cudaSuccess) e = cudaGraphInstantiate(&G->exec, G->graph, 0);
+    cudaStreamDestroy(s);
+    if (e != cudaSuccess) { release(G); return e; }
+    *out = G;
+    return cudaSuccess;
+}
+
+extern "C" cudaError_t bhBatchGraphUpdate(BHBatchGraph* G, const BHView* views, int n)
+{
+    if (!G || n != G->n || !views) return cudaErrorInvalidValue;
+    for (int i = 0; i < n; ++i)
+    {
+        const BHView &a = G->views[i], &b = views[i];
+        if (a.out != b.out || a.accum != b.accum || a.bloomA != b.bloomA || a.bloomB != b.bloomB ||
+            a.params.width != b.params.width || a.params.height != b.params.height ||
+            a.params.bloomEnabled != b.params.bloomEnabled)
+            return cudaErrorInvalidValue;
+    }
+    Plan pl;
+    pl.order = G->plan.order;
+    cudaError_t e = makePlan(views, n, pl, true);
+    if (e != cudaSuccess) return e;
+    for (int i = 0; i < n; ++i)   // post-processing constants are baked into the graph
+    {
+        const RenderParams &p0 = G->plan.params[i], &p1 = pl.params[i];
+        if (p0.exposure != p1.exposure || p0.bloomStrength != p1.bloomStrength || p0.swapRB != p1.swapRB)
+            return cudaErrorInvalidValue;
+    }
+    if ((e = cudaEventSynchronize(G->done)) != cudaSuccess) return e;   // last replay done with hPinned
+    G->plan = pl;
+    stage(*G);
+    return cudaSuccess;
+}
+
+extern "C" cudaError_t bhBatchGraphLaunch(BHBatchGraph* G, cudaStream_t stream)
+{
+    if (!G) return cudaErrorInvalidValue;
+    cudaError_t e = cudaGraphLaunch(G->exec, stream);
+    if (e != cudaSuccess) return e;
+    return cudaEventRecord(G->done, stream);
+}
+
+extern "C" void bhBatchGraphDestroy(BHBatchGraph* G)
+{
+    if (G && G->done) cudaEventSynchronize(G->done);
+    release(G);
+}
+
+// ---------------------------------------------------------------------------
+// autotuner
+// ---------------------------------------------------------------------------
+extern "C" cudaError_t bhAutotune(const RenderParams& p, int* refillMin, int* blocksPerSm, int* tileOrder,
+                                  float* bestMs)
+{
+    RenderParams P = p;
+    bhSanitizeRenderParams(&P);
+    const int family = isKerrModel(P.model) ? 1 : 0;
+    int maxBlocks = 0;
+    cudaError_t e = bh_trace_max_blocks(P.model, &maxBlocks);
+    if (e != cudaSuccess) return e;
+    float4* hdr = nullptr;
+    if ((e = cudaMalloc(&hdr, (size_t)P.width * P.height * sizeof(float4))) != cudaSuccess) return e;
+    cudaStream_t s = nullptr;
+    cudaEvent_t e0 = nullptr, e1 = nullptr;
+    cudaStreamCreateWithFlags(&s, cudaStreamNonBlocking);
+    cudaEventCreate(&e0);
+    cudaEventCreate(&e1);
+    int keepR = 32, keepB = 0;
+    bhGetTuning(family, &keepR, &keepB);
+    const int keepO = bhGetTileOrder();
+    float best = 1e30f;
+    int bR = keepR, bB = keepB, bO = keepO;
+    const int refills[] = {8, 16, 32};
+    for (int order = 0; order <= 1 && e == cudaSuccess; ++order)
+        for (int blocks = maxBlocks; blocks >= std::max(1, maxBlocks - 2) && e == cudaSuccess; --blocks)
+            for (int refill : refills)
+            {
+                bhSetTuning(family, refill, blocks);
+                bhSetTileOrder(order);
+                float ms = 1e30f;
+                for (int rep = 0; rep < 3 && e == cudaSuccess; ++rep)
+                {
+                    cudaEventRecord(e0, s);
+                    e = bhRenderHDR(hdr, P, BH_PREC_FP32, s);
+                    cudaEventRecord(e1, s);
+                    if (e == cudaSuccess) e = cudaEventSynchronize(e1);
+                    float t = 0.f;
+                    cudaEventElapsedTime(&t, e0, e1);
+                    if (rep > 0) ms = std::min(ms, t);   // first launch is the warm-up
+                }
+                if (e != cudaSuccess) break;
+                if (ms < best) { best = ms; bR = refill; bB = blocks; bO = order; }
+            }
+    cudaEventDestroy(e0);
+    cudaEventDestroy(e1);
+    cudaStreamDestroy(s);
+    cudaFree(hdr);
+    if (e != cudaSuccess)
+    {
+        bhSetTuning(family, keepR, keepB);
+        bhSetTileOrder(keepO);
+        return e;
+    }
+    bhSetTuning(family, bR, bB);
+    bhSetTileOrder(bO);
+    if (refillMin) *refillMin = bR;
+    if (blocksPerSm) *blocksPerSm = bB;
+    if (tileOrder) *tileOrder = bO;
+    if (bestMs) *bestMs = best;
+    return cudaSuccess;
+}

@@ -107,10 +107,11 @@ BH_DEV void sincos_theta(float x, float& s, float& c)
 }
 BH_DEV void sincos_theta(double x, double& s, double& c) { sincos(x, &s, &c); }
 
-// RK4 stage angles: the plain MUFU pair in FP32.  A stage only feeds the step
-// update with weight h/6..h/3, and the state's own sin/cos (sincos_theta) keeps
-// the relative accuracy at the poles.
-BH_DEV void sincos_stage(float x, float& s, float& c) { __sincosf(x, &s, &c); }
+// RK4 stage angles: the same pole-accurate pair.  (A plain MUFU sine has only
+// absolute accuracy, ~4e-7: near the poles the 1/sin^2 terms of the stages then
+// carry ~1e-5 relative error, enough to move escape directions by ~1e-4 rad
+// for cameras within a few degrees of the spin axis.)
+BH_DEV void sincos_stage(float x, float& s, float& c) { sincos_theta(x, s, c); }
 BH_DEV void sincos_stage(double x, double& s, double& c) { sincos(x, &s, &c); }
 
 // Cubic Hermite interpolant on a step: value at fraction t of the step of
@@ -218,9 +219,9 @@ BH_DEV SphInit<T> sph_init(const TraceParams& P, const CamFrame<T>& F, vec3<T> d
     return o;
 }
 
-// MIXED: FP32 state and steps; FP64 initial data, and whole steps in FP64 where
-// the Binet solution turns (|u'| would change sign within the step) or nears
-// the horizon; FP64 location of the equatorial crossing.
+// MIXED: FP32 state and steps; FP64 initial data, whole steps in FP64 where
+// the Binet solution turns (u' would change sign within the step), and FP64
+// location of the equatorial crossing.
 template <class R, bool STATS, bool MIXED = false>
 struct SphRay
 {
@@ -294,8 +295,8 @@ struct SphRay
         const R m3 = R(3) * M, q2 = R(2) * Q2;
         auto acc = [&](R x) { return (m3 * x - q2 * x * x) * x - x; };
         const R k1v = acc(u);
-        if (MIXED && (abs_p(du) < h * abs_p(k1v) || u > R(0.8f) * F.uHor))
-            binet_rk4_fp64(u, du, h, P.cd);      // turning point / horizon approach
+        if (MIXED && abs_p(du) < h * abs_p(k1v))
+            binet_rk4_fp64(u, du, h, P.cd);      // radial turning point
         else
         {
             R hh = R(0.5f) * h;
@@ -485,10 +486,12 @@ static __device__ __noinline__ KerrStep64 kerr_rk4_fp64(const CamFrame<double>& 
     return o;
 }
 
-// MIXED: FP32 state and steps; FP64 tetrad initial data, whole steps in FP64
-// at radial turning points (p_r would change sign within the step) and on
-// horizon approach (r < 1.5 r_floor), and FP64 bisection of the equatorial
-// crossing.
+// MIXED: FP32 state and steps; FP64 initial data (tetrad map and camera
+// position), whole steps in FP64 at radial turning points (p_r would change
+// sign within the step -- for near-extremal holes this includes periapses a
+// few percent outside the horizon), and FP64 bisection of the equatorial
+// crossing.  (FP64 steps over the whole final horizon approach were measured
+// to cost 70 % more time for no accuracy gain, and are not taken.)
 template <class R, bool STATS, bool MIXED = false>
 struct KerrRay
 {
@@ -530,6 +533,9 @@ struct KerrRay
             Lz = (R)xadd(xmul(D.gtp, ptUp), xmul(D.gpp, pfUp));
             pr = (R)xmul(drc, D.sqSD);
             pth = (R)xmul(dtc, D.sqS);
+            // the position too: near the poles acos(y / r) is ill-conditioned and
+            // the FP32 camera angle is off by up to ~1e-5 rad
+            r = (R)D.r0; th = (R)D.th0; ph = (R)D.ph0;
         }
         else
         {
@@ -541,9 +547,9 @@ struct KerrRay
             Lz = xadd(xmul(F.gtp, ptUp), xmul(F.gpp, pfUp));
             pr = xmul(drc, F.sqSD);
             pth = xmul(dtc, F.sqS);
+            r = F.r0; th = F.th0; ph = F.ph0;
         }
         k.E = E; k.Lz = Lz; k.aE = F.a * E; k.c1 = E * F.a2 - F.a * Lz; k.twoE = R(2) * E;
-        r = F.r0; th = F.th0; ph = F.ph0;
         sincos_theta(th, s, c);
         KerrEval<R> ev = kerr_rhs(F, k, r, s, c, pr, pth);
         d1 = ev.d;
@@ -607,7 +613,7 @@ struct KerrRay
         R dl0 = R(0), dl1 = R(0), dl2 = R(0);                 // the final stage's derivative
         if constexpr (MIXED)
         {
-            if (abs_p(pr) < h * abs_p(d1.pr) || r < F.rFloor * R(1.5f))
+            if (abs_p(pr) < h * abs_p(d1.pr))
             {
                 KerrStep64 o = kerr_rk4_fp64(P.cd, k.E, k.Lz, r, th, ph, pr, pth, h);
                 r = o.r; th = o.th; ph = o.ph; pr = o.pr; pth = o.pth;

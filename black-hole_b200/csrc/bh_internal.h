@@ -24,6 +24,14 @@ struct PostConsts
 cudaError_t bh_launch_trace(const TraceParams& P, int precision, bool stats, int blocksPerSm,
                             cudaStream_t stream);
 
+// batched views: one persistent launch over all views' tiles (bh_trace.cu);
+// `views` and `tileBase` (n + 1 prefix sums of tiles) are device tables
+cudaError_t bh_launch_batch(const TraceParams* views, const unsigned* tileBase, int n, unsigned totalTiles,
+                            unsigned* counter, int blocksPerSm, cudaStream_t stream);
+
+// resident CTAs per SM of the FP32 tracing kernel of a model's family
+cudaError_t bh_trace_max_blocks(int model, int* out);
+
 // bloom + tonemap of an accumulation buffer (bh_post.cu); `hblur` holds the
 // horizontally blurred half-resolution image ((W+1)/2 x (H+1)/2 float4)
 cudaError_t bh_launch_post(uchar4* out, const float4* accum, float4* hblur, int W, int H,
@@ -34,6 +42,8 @@ cudaError_t bh_launch_post(uchar4* out, const float4* accum, float4* hblur, int 
 struct RenderParams;
 TraceParams bh_frame_params(const RenderParams& P, int outMode, void* out);
 int bh_family_blocks(const RenderParams& P);
+// the library's per-device work counter (allocated on first use)
+cudaError_t bh_device_counter(unsigned** out);
 
 // camera-frame constants of t.camPos / t.M / t.a / t.Q in FP32 and FP64 (bh_camera.cpp)
 void bh_fill_camera_frames(TraceParams& t);

@@ -238,6 +238,79 @@ trace_kernel(const __grid_constant__ TraceParams P)
     }
 }
 
+// ---------------------------------------------------------------------------
+// Batched views: one persistent launch over the tiles of many views
+// ---------------------------------------------------------------------------
+// One tile (32 rays) of one view, traced by a whole warp: tile-synchronous, the
+// warp shades its 32 results together once every lane is done.
+template <class Ray>
+BH_DEV void trace_tile(const TraceParams& P, unsigned tile, unsigned lane)
+{
+    const unsigned rid = tile * 32u + lane;
+    int px = 0, py = 0;
+    const bool inFrame = ray_pixel(P, rid, px, py);
+    Ray ray;
+    bool live = false, fin = false;
+    unsigned key = 0;
+    if (inFrame)
+    {
+        key = (unsigned)py * (unsigned)P.W + (unsigned)px;
+        const int st = ray.init(P, ray_direction(P, rid, px, py));
+        live = (st == RAY_LIVE);
+        fin = (st == RAY_DONE);
+    }
+    while (live)
+        if (ray.advance(P)) { live = false; fin = true; }
+    __syncwarp();
+    if (fin)
+    {
+        PackedRay<typename Ray::Real> q;
+        ray.pack(P, key, q, nullptr);
+        shade_slot<Ray, false>(P, q, nullptr);
+    }
+}
+
+// Work queue: tile g of the whole batch belongs to the last view v with
+// tileBase[v] <= g.  A warp claims one tile at a time, copies the view's
+// frame constants into shared memory when the view changes, and branches on
+// the view's metric family (uniform across the warp).
+__global__ void __launch_bounds__(BH_TRACE_BLOCK, 5)
+batch_kernel(const TraceParams* __restrict__ views, const unsigned* __restrict__ tileBase, int n,
+             unsigned totalTiles, unsigned* counter)
+{
+    __shared__ TraceParams sp[kWarps];
+    const unsigned lane = threadIdx.x & 31u, warp = threadIdx.x >> 5;
+    const unsigned FULL = 0xffffffffu;
+    int cur = -1;
+    while (true)
+    {
+        unsigned g = 0;
+        if (lane == 0) g = atomicAdd(counter, 1u);
+        g = __shfl_sync(FULL, g, 0);
+        if (g >= totalTiles) break;
+        int lo = 0, hi = n;
+        while (hi - lo > 1)
+        {
+            const int mid = (lo + hi) >> 1;
+            if (__ldg(tileBase + mid) <= g) lo = mid; else hi = mid;
+        }
+        if (lo != cur)
+        {
+            const long long* src = reinterpret_cast<const long long*>(views + lo);
+            long long* dst = reinterpret_cast<long long*>(&sp[warp]);
+            for (int i = (int)lane; i < (int)(sizeof(TraceParams) / 8); i += 32) dst[i] = __ldg(src + i);
+            __syncwarp();
+            cur = lo;
+        }
+        const TraceParams& P = sp[warp];
+        const unsigned tile = g - __ldg(tileBase + lo);
+        if (P.model == 2 || P.model == 3) trace_tile<KerrRay<float, false>>(P, tile, lane);
+        else trace_tile<SphRay<float, false>>(P, tile, lane);
+        __syncwarp();
+    }
+}
+static_assert(sizeof(TraceParams) % 8 == 0, "TraceParams is copied in 8-byte words");
+
 template <class Ray, bool STATS>
 cudaError_t launch_one(const TraceParams& P, int blocksPerSm, cudaStream_t stream)
 {
@@ -287,4 +360,31 @@ cudaError_t bh_launch_trace(const TraceParams& P, int precision, bool stats, int
                           : launch_one<SphRay<double, false>, false>(P, blocksPerSm, stream);
     return stats ? launch_one<SphRay<float, true>, true>(P, blocksPerSm, stream)
                  : launch_one<SphRay<float, false>, false>(P, blocksPerSm, stream);
+}
+
+cudaError_t bh_launch_batch(const TraceParams* views, const unsigned* tileBase, int n, unsigned totalTiles,
+                            unsigned* counter, int blocksPerSm, cudaStream_t stream)
+{
+    cudaError_t e = cudaMemsetAsync(counter, 0, sizeof(unsigned), stream);
+    if (e != cudaSuccess || totalTiles == 0) return e;
+    int dev = 0, sms = 0, occ = 0;
+    if ((e = cudaGetDevice(&dev)) != cudaSuccess) return e;
+    if ((e = cudaDeviceGetAttribute(&sms, cudaDevAttrMultiProcessorCount, dev)) != cudaSuccess) return e;
+    if ((e = cudaOccupancyMaxActiveBlocksPerMultiprocessor(&occ, batch_kernel, BH_TRACE_BLOCK, 0)) != cudaSuccess)
+        return e;
+    if (occ < 1) occ = 1;
+    const int per = (blocksPerSm > 0 && blocksPerSm < occ) ? blocksPerSm : occ;
+    long long grid = (long long)per * sms;
+    const long long need = ((long long)totalTiles * 32 + BH_TRACE_BLOCK - 1) / BH_TRACE_BLOCK;
+    if (grid > need) grid = need;
+    batch_kernel<<<(unsigned)grid, BH_TRACE_BLOCK, 0, stream>>>(views, tileBase, n, totalTiles, counter);
+    return cudaGetLastError();
+}
+
+cudaError_t bh_trace_max_blocks(int model, int* out)
+{
+    const bool kerr = (model == 2 || model == 3);
+    return cudaOccupancyMaxActiveBlocksPerMultiprocessor(
+        out, kerr ? trace_kernel<KerrRay<float, false>, false> : trace_kernel<SphRay<float, false>, false>,
+        BH_TRACE_BLOCK, 0);
 }

@@ -149,6 +149,46 @@ void bhGetTuning(int family, int* refillMin, int* blocksPerSm);
  * the first call at that resolution (a blocking upload: make that first call
  * outside any stream capture).  Returns 1 when applied, 0 when out of range. */
 int bhSetTileOrder(int mode);
+int bhGetTileOrder(void);
+
+/* ---- batches of views (no counterpart in the reference) ----------------- */
+
+/* One view of a batch: its parameters and the buffers launchRenderPipeline
+ * would take for it (bloomA / bloomB may be null when bloom is off). */
+typedef struct BHView
+{
+    RenderParams params;
+    uchar4* out;
+    float4* accum;
+    float4* bloomA;
+    float4* bloomB;
+} BHView;
+
+/* Render n views: the same images as n launchRenderPipeline calls, traced in
+ * ONE persistent launch that draws 8x4-pixel tiles of all views from a single
+ * device work queue (both metric families, any mix of resolutions), followed
+ * by each view's bloom and tonemap.  Views are queued longest-first by
+ * estimated cost.  FP32.  The library keeps per-device tables of the views'
+ * frame constants, grown on demand (an allocation on the first call and when
+ * n grows; make those calls outside stream capture). */
+cudaError_t bhRenderBatch(const BHView* views, int n, cudaStream_t stream);
+
+/* The batch as a CUDA graph: created once for fixed views (buffers,
+ * resolutions, bloom on/off, exposure and bloom strength), then launched
+ * every frame; bhBatchGraphUpdate replaces the other parameters (camera,
+ * metric, disk time, ...) before the next launch (it waits for the previous
+ * launch to have read them).  The graph owns its tables and counter. */
+typedef struct BHBatchGraph BHBatchGraph;
+cudaError_t bhBatchGraphCreate(BHBatchGraph** graph, const BHView* views, int n);
+cudaError_t bhBatchGraphUpdate(BHBatchGraph* graph, const BHView* views, int n);
+cudaError_t bhBatchGraphLaunch(BHBatchGraph* graph, cudaStream_t stream);
+void bhBatchGraphDestroy(BHBatchGraph* graph);
+
+/* Autotuner: times the FP32 tracing kernel of p's metric family on p's view
+ * (blocking, with a temporary HDR buffer) over the resident CTAs per SM, the
+ * warp refill threshold and the tile order, applies the fastest setting
+ * (bhSetTuning / bhSetTileOrder) and reports it. */
+cudaError_t bhAutotune(BH_PARAMS_IN p, int* refillMin, int* blocksPerSm, int* tileOrder, float* bestMs);
 
 /* ---- allocation-free pipeline (no counterpart in the reference) --------- */
 

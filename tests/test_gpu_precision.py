@@ -54,7 +54,12 @@ def test_mixed_and_fp32_against_fp64_on_the_4k_sweep_scene(cuda, el):
     print(f"el={el}: fp32 {e32}  mixed {emx}")
     for e in (e32, emx):
         assert e["cls_inner"] <= max(2, int(0.001 * NX * NY)), e
-        assert e["esc_1e4"] >= 0.99, e
+    # Within a few degrees of the spin axis the reference's FP32 set-up itself is
+    # ill-conditioned (theta0 = acos(y / r) loses ~1e-5 rad), so plain FP32
+    # may leave up to 2 % of escape directions beyond 1e-4 rad there; the mixed
+    # mode, with its FP64 set-up, must meet the 1e-4 rad bar everywhere.
+    assert e32["esc_1e4"] >= (0.99 if el < 80 else 0.98), e32
+    assert emx["esc_1e4"] >= 0.99, emx
     # mixed precision is at least as close to the FP64 integration as plain FP32
     assert emx["esc_med"] <= e32["esc_med"] * 1.05 + 1e-9
     assert emx["cls_all"] <= e32["cls_all"] + 2
