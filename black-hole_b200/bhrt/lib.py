@@ -40,6 +40,7 @@ _SIGNATURES = {
     "bhBatchGraphLaunch": (_int, [_vp, _vp]),
     "bhBatchGraphDestroy": (None, [_vp]),
     "bhAutotune": (_int, [_P, C.POINTER(_int), C.POINTER(_int), C.POINTER(_int), C.POINTER(C.c_float)]),
+    "bhAutotuneBatch": (_int, [_vp, _int, C.POINTER(_int), C.POINTER(_int), C.POINTER(C.c_float)]),
     "bhRenderPipelineNoAlloc": (_int, [_vp, _vp, _P, _vp]),
     "bhMeasureFp32Peak": (C.c_double, []),
     "bhVersion": (C.c_char_p, []),

@@ -5,11 +5,13 @@
 // No counterpart in the reference, which renders one view per call
 // (src/black_hole_kernel.cu:108-134).  A batch is equivalent to calling
 // launchRenderPipeline for every view in turn: same sanitising, same images.
-// What changes is scheduling: every view's 8x4-pixel tiles go into one device
-// work queue, traced by one persistent kernel (bh_trace.cu, batch_kernel), so
-// small views, large views and both metric families share the GPU with no
-// per-view launch gaps or tails.  Views are queued in order of estimated cost
-// (pixels x family factor), longest first, so the batch ends on cheap tiles.
+// What changes is scheduling: the 8x4-pixel tiles of all views of a metric
+// family go into one device work queue, traced by one persistent kernel
+// (bh_trace.cu, batch_kernel), so small and large views share the GPU with no
+// per-view launch gaps or tails.  Two launches per batch (Kerr family, then
+// the spherical metrics), each with its family's register budget; the gap
+// between them is one tile's duration.  Within a family views are queued by
+// pixel count, largest first, so each queue ends on cheap tiles.
 // ---------------------------------------------------------------------------
 #include <algorithm>
 #include <mutex>
@@ -24,10 +26,11 @@ bool isKerrModel(int m) { return m == BH_KERR || m == BH_KERR_NEWMAN; }
 
 struct Plan
 {
-    std::vector<int> order;               // trace position -> view index
+    std::vector<int> order;               // trace position -> view index (Kerr family first)
     std::vector<RenderParams> params;     // sanitised, by view index
     std::vector<TraceParams> table;       // trace order
-    std::vector<unsigned> base;           // n + 1 tile prefix sums, trace order
+    std::vector<unsigned> base;           // per family, tile prefix sums: nKerr + 1, then nSph + 1
+    int nKerr = 0;
 };
 
 cudaError_t checkView(const BHView& v, const RenderParams& P)
@@ -54,14 +57,18 @@ cudaError_t makePlan(const BHView* views, int n, Plan& pl, bool keepOrder)
     {
         pl.order.resize(n);
         for (int i = 0; i < n; ++i) pl.order[i] = i;
-        auto cost = [&](int i) {
+        auto key = [&](int i) {
             const RenderParams& P = pl.params[i];
-            return (double)P.width * P.height * (isKerrModel(P.model) ? 3.0 : 1.0);
+            return (isKerrModel(P.model) ? 1e12 : 0.0) + (double)P.width * P.height;
         };
-        std::stable_sort(pl.order.begin(), pl.order.end(), [&](int a, int b) { return cost(a) > cost(b); });
+        std::stable_sort(pl.order.begin(), pl.order.end(), [&](int a, int b) { return key(a) > key(b); });
     }
+    pl.nKerr = 0;
+    for (int k = 0; k < n; ++k) pl.nKerr += isKerrModel(pl.params[pl.order[k]].model) ? 1 : 0;
+    for (int k = 0; k < n; ++k)   // a kept order must still put the Kerr family first
+        if (isKerrModel(pl.params[pl.order[k]].model) != (k < pl.nKerr)) return cudaErrorInvalidValue;
     pl.table.resize(n);
-    pl.base.assign(n + 1, 0u);
+    pl.base.assign(n + 2, 0u);
     for (int k = 0; k < n; ++k)
     {
         const int i = pl.order[k];
@@ -70,7 +77,8 @@ cudaError_t makePlan(const BHView* views, int n, Plan& pl, bool keepOrder)
         t.counter = nullptr;
         pl.table[k] = t;
         const unsigned tiles = (unsigned)t.tilesX * (unsigned)((t.H + 3) / 4);
-        pl.base[k + 1] = pl.base[k] + tiles;
+        const int b = k < pl.nKerr ? k : k + 1;   // the spherical prefix sums start at nKerr + 1
+        pl.base[b + 1] = pl.base[b] + tiles;
     }
     return cudaSuccess;
 }
@@ -78,11 +86,16 @@ cudaError_t makePlan(const BHView* views, int n, Plan& pl, bool keepOrder)
 cudaError_t launchPlan(const Plan& pl, const BHView* views, const TraceParams* dTable, const unsigned* dBase,
                        unsigned* counter, cudaStream_t s)
 {
-    const int n = (int)pl.table.size();
-    int blocks = 0;
-    bhGetTuning(1, nullptr, &blocks);
-    cudaError_t e = bh_launch_batch(dTable, dBase, n, pl.base[n], counter, blocks, s);
-    if (e != cudaSuccess) return e;
+    const int n = (int)pl.table.size(), nK = pl.nKerr, nS = n - nK;
+    int blocksK = 0, blocksS = 0;
+    bhGetTuning(1, nullptr, &blocksK);
+    bhGetTuning(0, nullptr, &blocksS);
+    cudaError_t e = cudaSuccess;
+    if (nK > 0 && (e = bh_launch_batch(true, dTable, dBase, nK, pl.base[nK], counter, blocksK, s)) != cudaSuccess)
+        return e;
+    if (nS > 0 && (e = bh_launch_batch(false, dTable + nK, dBase + nK + 1, nS, pl.base[n + 1], counter, blocksS,
+                                       s)) != cudaSuccess)
+        return e;
     for (int i = 0; i < n; ++i)
     {
         const RenderParams& P = pl.params[i];
@@ -120,7 +133,7 @@ cudaError_t ensureTables(int n, DevTables** out)
         t.cap = 0;
         size_t cap = std::max<size_t>(64, (size_t)n);
         if ((e = cudaMalloc(&t.table, cap * sizeof(TraceParams))) != cudaSuccess) return e;
-        if ((e = cudaMalloc(&t.base, (cap + 1) * sizeof(unsigned))) != cudaSuccess) return e;
+        if ((e = cudaMalloc(&t.base, (cap + 2) * sizeof(unsigned))) != cudaSuccess) return e;
         t.cap = cap;
     }
     *out = &t;
@@ -145,7 +158,7 @@ extern "C" cudaError_t bhRenderBatch(const BHView* views, int n, cudaStream_t st
     // pageable sources: the copies are staged before the calls return
     if ((e = cudaMemcpyAsync(t->table, pl.table.data(), n * sizeof(TraceParams), cudaMemcpyHostToDevice, stream)))
         return e;
-    if ((e = cudaMemcpyAsync(t->base, pl.base.data(), (n + 1) * sizeof(unsigned), cudaMemcpyHostToDevice, stream)))
+    if ((e = cudaMemcpyAsync(t->base, pl.base.data(), (n + 2) * sizeof(unsigned), cudaMemcpyHostToDevice, stream)))
         return e;
     return launchPlan(pl, views, t->table, t->base, counter, stream);
 }
@@ -175,7 +188,7 @@ void stage(BHBatchGraph& G)
     std::copy(reinterpret_cast<const unsigned char*>(G.plan.table.data()),
               reinterpret_cast<const unsigned char*>(G.plan.table.data()) + tb, G.hPinned);
     std::copy(reinterpret_cast<const unsigned char*>(G.plan.base.data()),
-              reinterpret_cast<const unsigned char*>(G.plan.base.data()) + (G.n + 1) * sizeof(unsigned),
+              reinterpret_cast<const unsigned char*>(G.plan.base.data()) + (G.n + 2) * sizeof(unsigned),
               G.hPinned + tb);
 }
 
@@ -203,7 +216,7 @@ extern "C" cudaError_t bhBatchGraphCreate(BHBatchGraph** out, const BHView* view
     G->views.assign(views, views + n);
     cudaError_t e = makePlan(views, n, G->plan, false);
     cudaStream_t s = nullptr;
-    const size_t tb = n * sizeof(TraceParams), bb = (n + 1) * sizeof(unsigned);
+    const size_t tb = n * sizeof(TraceParams), bb = (n + 2) * sizeof(unsigned);
     if (e == cudaSuccess) e = cudaGetDevice(&G->device);
     if (e == cudaSuccess) e = cudaMalloc(&G->dTable, tb);
     if (e == cudaSuccess) e = cudaMalloc(&G->dBase, bb);
@@ -332,4 +345,55 @@ extern "C" cudaError_t bhAutotune(const RenderParams& p, int* refillMin, int* bl
     if (tileOrder) *tileOrder = bO;
     if (bestMs) *bestMs = best;
     return cudaSuccess;
+}
+
+extern "C" cudaError_t bhAutotuneBatch(const BHView* views, int n, int* blocksKerr, int* blocksSph, float* bestMs)
+{
+    Plan pl;
+    cudaError_t e = makePlan(views, n, pl, false);
+    if (e != cudaSuccess) return e;
+    cudaStream_t s = nullptr;
+    cudaEvent_t e0 = nullptr, e1 = nullptr;
+    if ((e = cudaStreamCreateWithFlags(&s, cudaStreamNonBlocking)) != cudaSuccess) return e;
+    cudaEventCreate(&e0);
+    cudaEventCreate(&e1);
+    float total = 0.f;
+    for (int family = 1; family >= 0 && e == cudaSuccess; --family)
+    {
+        std::vector<BHView> sub;
+        for (int k = 0; k < n; ++k)
+            if ((k < pl.nKerr) == (family == 1)) sub.push_back(views[pl.order[k]]);
+        if (sub.empty()) continue;
+        int maxBlocks = 0, keepR = 32, keepB = 0;
+        if ((e = bh_trace_max_blocks(family ? BH_KERR : BH_SCHWARZSCHILD, &maxBlocks)) != cudaSuccess) break;
+        bhGetTuning(family, &keepR, &keepB);
+        float best = 1e30f;
+        int bestB = keepB;
+        for (int blocks = maxBlocks; blocks >= std::max(1, maxBlocks - 2) && e == cudaSuccess; --blocks)
+        {
+            bhSetTuning(family, keepR, blocks);
+            float ms = 1e30f;
+            for (int rep = 0; rep < 3 && e == cudaSuccess; ++rep)
+            {
+                cudaEventRecord(e0, s);
+                e = bhRenderBatch(sub.data(), (int)sub.size(), s);
+                cudaEventRecord(e1, s);
+                if (e == cudaSuccess) e = cudaEventSynchronize(e1);
+                float t = 0.f;
+                cudaEventElapsedTime(&t, e0, e1);
+                if (rep > 0) ms = std::min(ms, t);   // first launch is the warm-up
+            }
+            if (e == cudaSuccess && ms < best) { best = ms; bestB = blocks; }
+        }
+        bhSetTuning(family, keepR, e == cudaSuccess ? bestB : keepB);
+        if (e != cudaSuccess) break;
+        total += best;
+        if (family == 1 && blocksKerr) *blocksKerr = bestB;
+        if (family == 0 && blocksSph) *blocksSph = bestB;
+    }
+    cudaEventDestroy(e0);
+    cudaEventDestroy(e1);
+    cudaStreamDestroy(s);
+    if (e == cudaSuccess && bestMs) *bestMs = total;
+    return e;
 }

@@ -24,10 +24,12 @@ struct PostConsts
 cudaError_t bh_launch_trace(const TraceParams& P, int precision, bool stats, int blocksPerSm,
                             cudaStream_t stream);
 
-// batched views: one persistent launch over all views' tiles (bh_trace.cu);
-// `views` and `tileBase` (n + 1 prefix sums of tiles) are device tables
-cudaError_t bh_launch_batch(const TraceParams* views, const unsigned* tileBase, int n, unsigned totalTiles,
-                            unsigned* counter, int blocksPerSm, cudaStream_t stream);
+// batched views of one metric family (`kerr`: Kerr / Kerr-Newman, else the
+// spherical metrics): zero the counter, then one persistent launch over all
+// the views' tiles (bh_trace.cu); `views` and `tileBase` (n + 1 prefix sums of
+// tiles) are device tables
+cudaError_t bh_launch_batch(bool kerr, const TraceParams* views, const unsigned* tileBase, int n,
+                            unsigned totalTiles, unsigned* counter, int blocksPerSm, cudaStream_t stream);
 
 // resident CTAs per SM of the FP32 tracing kernel of a model's family
 cudaError_t bh_trace_max_blocks(int model, int* out);

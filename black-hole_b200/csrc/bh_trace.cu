@@ -270,11 +270,12 @@ BH_DEV void trace_tile(const TraceParams& P, unsigned tile, unsigned lane)
     }
 }
 
-// Work queue: tile g of the whole batch belongs to the last view v with
-// tileBase[v] <= g.  A warp claims one tile at a time, copies the view's
-// frame constants into shared memory when the view changes, and branches on
-// the view's metric family (uniform across the warp).
-__global__ void __launch_bounds__(BH_TRACE_BLOCK, 5)
+// Work queue: tile g of the batch belongs to the last view v with
+// tileBase[v] <= g.  A warp claims one tile at a time and copies the view's
+// frame constants into shared memory when the view changes.  One kernel per
+// metric family, so each runs with its family's register budget.
+template <class Ray>
+__global__ void __launch_bounds__(BH_TRACE_BLOCK, min_blocks<Ray, false>())
 batch_kernel(const TraceParams* __restrict__ views, const unsigned* __restrict__ tileBase, int n,
              unsigned totalTiles, unsigned* counter)
 {
@@ -302,10 +303,7 @@ batch_kernel(const TraceParams* __restrict__ views, const unsigned* __restrict__
             __syncwarp();
             cur = lo;
         }
-        const TraceParams& P = sp[warp];
-        const unsigned tile = g - __ldg(tileBase + lo);
-        if (P.model == 2 || P.model == 3) trace_tile<KerrRay<float, false>>(P, tile, lane);
-        else trace_tile<SphRay<float, false>>(P, tile, lane);
+        trace_tile<Ray>(sp[warp], g - __ldg(tileBase + lo), lane);
         __syncwarp();
     }
 }
@@ -362,22 +360,22 @@ cudaError_t bh_launch_trace(const TraceParams& P, int precision, bool stats, int
                  : launch_one<SphRay<float, false>, false>(P, blocksPerSm, stream);
 }
 
-cudaError_t bh_launch_batch(const TraceParams* views, const unsigned* tileBase, int n, unsigned totalTiles,
-                            unsigned* counter, int blocksPerSm, cudaStream_t stream)
+cudaError_t bh_launch_batch(bool kerr, const TraceParams* views, const unsigned* tileBase, int n,
+                            unsigned totalTiles, unsigned* counter, int blocksPerSm, cudaStream_t stream)
 {
     cudaError_t e = cudaMemsetAsync(counter, 0, sizeof(unsigned), stream);
     if (e != cudaSuccess || totalTiles == 0) return e;
+    auto k = kerr ? batch_kernel<KerrRay<float, false>> : batch_kernel<SphRay<float, false>>;
     int dev = 0, sms = 0, occ = 0;
     if ((e = cudaGetDevice(&dev)) != cudaSuccess) return e;
     if ((e = cudaDeviceGetAttribute(&sms, cudaDevAttrMultiProcessorCount, dev)) != cudaSuccess) return e;
-    if ((e = cudaOccupancyMaxActiveBlocksPerMultiprocessor(&occ, batch_kernel, BH_TRACE_BLOCK, 0)) != cudaSuccess)
-        return e;
+    if ((e = cudaOccupancyMaxActiveBlocksPerMultiprocessor(&occ, k, BH_TRACE_BLOCK, 0)) != cudaSuccess) return e;
     if (occ < 1) occ = 1;
     const int per = (blocksPerSm > 0 && blocksPerSm < occ) ? blocksPerSm : occ;
     long long grid = (long long)per * sms;
     const long long need = ((long long)totalTiles * 32 + BH_TRACE_BLOCK - 1) / BH_TRACE_BLOCK;
     if (grid > need) grid = need;
-    batch_kernel<<<(unsigned)grid, BH_TRACE_BLOCK, 0, stream>>>(views, tileBase, n, totalTiles, counter);
+    k<<<(unsigned)grid, BH_TRACE_BLOCK, 0, stream>>>(views, tileBase, n, totalTiles, counter);
     return cudaGetLastError();
 }
 

@@ -164,20 +164,23 @@ typedef struct BHView
     float4* bloomB;
 } BHView;
 
-/* Render n views: the same images as n launchRenderPipeline calls, traced in
- * ONE persistent launch that draws 8x4-pixel tiles of all views from a single
- * device work queue (both metric families, any mix of resolutions), followed
- * by each view's bloom and tonemap.  Views are queued longest-first by
- * estimated cost.  FP32.  The library keeps per-device tables of the views'
- * frame constants, grown on demand (an allocation on the first call and when
- * n grows; make those calls outside stream capture). */
+/* Render n views: the same images as n launchRenderPipeline calls, traced by
+ * one persistent launch per metric family (Kerr / Kerr-Newman, then
+ * Schwarzschild / Reissner-Nordstrom) that draws 8x4-pixel tiles of all the
+ * family's views, any mix of resolutions, from a single device work queue,
+ * followed by each view's bloom and tonemap.  Within a family views are queued
+ * largest first.  FP32; CTAs per SM from bhSetTuning of each family.  The
+ * library keeps per-device tables of the views' frame constants, grown on
+ * demand (an allocation on the first call and when n grows; make those calls
+ * outside stream capture). */
 cudaError_t bhRenderBatch(const BHView* views, int n, cudaStream_t stream);
 
 /* The batch as a CUDA graph: created once for fixed views (buffers,
- * resolutions, bloom on/off, exposure and bloom strength), then launched
- * every frame; bhBatchGraphUpdate replaces the other parameters (camera,
- * metric, disk time, ...) before the next launch (it waits for the previous
- * launch to have read them).  The graph owns its tables and counter. */
+ * resolutions, bloom on/off, exposure, bloom strength and metric family),
+ * then launched every frame; bhBatchGraphUpdate replaces the other parameters
+ * (camera, spin, charge, disk time, ...) before the next launch (it waits for
+ * the previous launch to have read them) and refuses changes to the fixed
+ * ones with cudaErrorInvalidValue.  The graph owns its tables and counter. */
 typedef struct BHBatchGraph BHBatchGraph;
 cudaError_t bhBatchGraphCreate(BHBatchGraph** graph, const BHView* views, int n);
 cudaError_t bhBatchGraphUpdate(BHBatchGraph* graph, const BHView* views, int n);
@@ -189,6 +192,13 @@ void bhBatchGraphDestroy(BHBatchGraph* graph);
  * warp refill threshold and the tile order, applies the fastest setting
  * (bhSetTuning / bhSetTileOrder) and reports it. */
 cudaError_t bhAutotune(BH_PARAMS_IN p, int* refillMin, int* blocksPerSm, int* tileOrder, float* bestMs);
+
+/* Batch autotuner: for each metric family present in the views, times
+ * bhRenderBatch on that family's views (blocking) over the resident CTAs per
+ * SM, applies the fastest (bhSetTuning; the refill threshold is kept) and
+ * reports it (blocksKerr / blocksSph are left unchanged for an absent family).
+ * bestMs = the two families' best times added. */
+cudaError_t bhAutotuneBatch(const BHView* views, int n, int* blocksKerr, int* blocksSph, float* bestMs);
 
 /* ---- allocation-free pipeline (no counterpart in the reference) --------- */
 

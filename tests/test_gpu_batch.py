@@ -100,9 +100,14 @@ def test_batch_graph_launch_and_update(cuda):
         assert L.bhBatchGraphLaunch(g, stream) == 0
         torch.cuda.synchronize()
         _check(bufs, _singles(moved))
-        # a changed resolution is refused
+        # a changed resolution, or a view moved to the other metric family, is refused
         bad = _view_array([params[0].copy()] + moved[1:], bufs)
         bad[0].params.width += 2
+        assert L.bhBatchGraphUpdate(g, bad, len(moved)) != 0
+        other = params[0].copy()
+        scenes.apply_black_hole(other, 2 if other.model < 2 else 0, 0.5 if other.model < 2 else 0.0, 0.0,
+                                lib.derive)
+        bad = _view_array([other] + moved[1:], bufs)
         assert L.bhBatchGraphUpdate(g, bad, len(moved)) != 0
     finally:
         L.bhBatchGraphDestroy(g)
@@ -121,3 +126,25 @@ def test_autotune_applies_a_valid_setting(cuda):
     finally:
         lib.set_tuning(1, *before[0])
         L.bhSetTileOrder(before[1])
+
+
+def test_batch_autotune_then_batch_still_matches(cuda):
+    L = lib.load()
+    params = _views(8, seed=3)
+    bufs = [_buffers(P) for P in params]
+    arr = _view_array(params, bufs)
+    bk, bs, ms = C.c_int(-1), C.c_int(-1), C.c_float()
+    before = lib.get_tuning(0), lib.get_tuning(1)
+    try:
+        assert L.bhAutotuneBatch(arr, len(params), C.byref(bk), C.byref(bs), C.byref(ms)) == 0
+        assert bk.value >= 1 and bs.value >= 1 and 0.0 < ms.value < 1e4
+        assert lib.get_tuning(1)[1] == bk.value and lib.get_tuning(0)[1] == bs.value
+        import torch
+        for b in bufs:
+            b["out"].zero_()
+        assert L.bhRenderBatch(arr, len(params), C.c_void_p(torch.cuda.current_stream().cuda_stream)) == 0
+        torch.cuda.synchronize()
+        _check(bufs, _singles(params))
+    finally:
+        lib.set_tuning(0, *before[0])
+        lib.set_tuning(1, *before[1])
