@@ -43,6 +43,8 @@ _SIGNATURES = {
     "bhAutotuneBatch": (_int, [_vp, _int, C.POINTER(_int), C.POINTER(_int), C.POINTER(C.c_float)]),
     "bhRenderPipelineNoAlloc": (_int, [_vp, _vp, _P, _vp]),
     "bhMeasureFp32Peak": (C.c_double, []),
+    "bhTcGemm": (_int, [_vp, _int, _vp, _int, _vp, _int, _int, _int, _int, _int, _int, _vp, _vp]),
+    "bhTcErrorFlags": (_int, [C.POINTER(C.c_uint)]),
     "bhVersion": (C.c_char_p, []),
 }
 
