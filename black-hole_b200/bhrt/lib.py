@@ -45,6 +45,20 @@ _SIGNATURES = {
     "bhMeasureFp32Peak": (C.c_double, []),
     "bhTcGemm": (_int, [_vp, _int, _vp, _int, _vp, _int, _int, _int, _int, _int, _int, _vp, _vp]),
     "bhTcErrorFlags": (_int, [C.POINTER(C.c_uint)]),
+    "bhSurrogateParamCount": (_int, []),
+    "bhSurrogateCreate": (_int, [C.POINTER(_vp), C.c_uint]),
+    "bhSurrogateDestroy": (None, [_vp]),
+    "bhSurrogateGetParams": (_int, [_vp, _vp]),
+    "bhSurrogateSetParams": (_int, [_vp, _vp]),
+    "bhSurrogateFeatures": (_int, [_vp, _vp, _int, _vp]),
+    "bhSurrogateForward": (_int, [_vp, _vp, _vp, _int, _int, _vp]),
+    "bhSurrogateGradients": (_int, [_vp, _vp, _vp, _int, _vp, _vp]),
+    "bhSurrogateGenerate": (_int, [_vp, C.c_longlong, _int, C.c_uint]),
+    "bhSurrogateDataset": (_int, [_vp, C.POINTER(_vp), C.POINTER(_vp), C.POINTER(C.c_longlong)]),
+    "bhSurrogateDatasetCopy": (_int, [_vp, _vp, _vp, C.c_longlong, C.c_longlong]),
+    "bhSurrogateTrain": (_int, [_vp, _int, _int, C.c_float, C.c_uint, _vp]),
+    "bhSurrogateRender": (_int, [_vp, _vp, _vp, _vp, _vp, _P, _vp]),
+    "bhSurrogateFrameStats": (_int, [_vp, _vp]),
     "bhVersion": (C.c_char_p, []),
 }
 

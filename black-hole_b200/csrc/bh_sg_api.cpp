@@ -1,0 +1,516 @@
+// ---------------------------------------------------------------------------
+// bh_sg_api.cpp -- C-ABI of the lensing surrogate (include/bh_surrogate_api.h):
+// the network object, the RK4-traced ray set, the training loop, and the
+// surrogate frame (fused inference -> RK4 for the rest -> held-out check ->
+// bloom and tonemap).
+// No counterpart in the reference (it has no learned component); the frames
+// it renders use the reference's camera, sky and post-processing exactly as
+// launchRenderPipeline does.
+// ---------------------------------------------------------------------------
+#include <cmath>
+#include <cstdint>
+#include <cstring>
+#include <random>
+#include <vector>
+#include <cuda_runtime.h>
+#include "bh_internal.h"
+#include "bh_launch.h"
+#include "bh_sg_infer.h"
+#include "bh_sg_train.h"
+#include "bh_surrogate.h"
+#include "bh_surrogate_api.h"
+
+namespace {
+
+constexpr int kHidW = 256 * 256;           // one hidden weight matrix
+constexpr int kWCount = 4 * kHidW + 256 * 64;
+constexpr int kBiasCount = 4 * 256 + 16;
+constexpr int kHeldStride = 256;
+constexpr float kPi = 3.14159265358979f;
+
+// uniform float in [lo, hi) from a 32-bit generator (portable, unlike std distributions)
+float uni(std::mt19937& g, float lo, float hi)
+{
+    return lo + (hi - lo) * (float)((double)g() * (1.0 / 4294967296.0));
+}
+
+struct CritKey
+{
+    int model = -1, maxSteps = 0;
+    float M = 0, a = 0, Q = 0, dist = 0, cosIncl = 0, tanHalfFov = 0, dPhi = 0;
+    bool operator==(const CritKey& o) const
+    {
+        return model == o.model && maxSteps == o.maxSteps && M == o.M && a == o.a && Q == o.Q && dist == o.dist &&
+               cosIncl == o.cosIncl && tanHalfFov == o.tanHalfFov && dPhi == o.dPhi;
+    }
+};
+
+float length3(const float3& v) { return std::sqrt(v.x * v.x + v.y * v.y + v.z * v.z); }
+
+// The orbit camera of the reference application (src/main.cpp:186-228): camera
+// at distance d, elevation el, azimuth az about the +Y spin axis, looking at
+// the hole, no body rotation.
+void orbitCamera(RenderParams& P, float az, float el, float d, float fovDeg)
+{
+    const float ca = std::cos(az), sa = std::sin(az), ce = std::cos(el), se = std::sin(el);
+    float3 p{d * ce * ca, d * se, d * ce * sa};
+    const float fl = length3(p);
+    float3 f{-p.x / fl, -p.y / fl, -p.z / fl};
+    float3 r{-f.z, 0.f, f.x};
+    float rl = std::sqrt(r.x * r.x + r.z * r.z);
+    if (rl < 1e-6f) { r = float3{1.f, 0.f, 0.f}; rl = 1.f; }
+    r = float3{r.x / rl, 0.f, r.z / rl};
+    float3 u{r.y * f.z - r.z * f.y, r.z * f.x - r.x * f.z, r.x * f.y - r.y * f.x};
+    const float ul = length3(u);
+    u = float3{u.x / ul, u.y / ul, u.z / ul};
+    P.camPos = p; P.camForward = f; P.camRight = r; P.camUp = u;
+    P.tanHalfFov = std::tan(fovDeg * kPi / 180.f * 0.5f);
+    P.aspect = (float)P.width / (float)P.height;
+}
+
+// applyBlackHole (src/main.cpp:97-134): derive, disk inner edge at the ISCO.
+void applyHole(RenderParams& P, int model, float aStar, float q)
+{
+    float M = 0.5f, a = aStar, qq = q;
+    BHDerived d;
+    bhValidateAndDerive(model, &M, &a, &qq, 0, &d);
+    P.model = model;
+    P.M = M;
+    P.aSpin = d.a; P.Qc = d.Q;
+    P.rPlus = d.rPlus; P.rPhoton = d.rPhoton; P.rErgo = d.rErgo;
+    P.allowNaked = 0;
+    P.diskInner = d.rIsco;
+    P.diskOuter = 8.f;
+}
+
+// normalised scene inputs of a sanitised orbit-camera frame
+void sceneInputs(const RenderParams& P, float& aN, float& qN, float& rN, float& iN)
+{
+    const float r = length3(P.camPos);
+    const float incl = std::acos(std::fmax(-1.f, std::fmin(1.f, P.camPos.y / r))) * 180.f / kPi;
+    aN = P.aSpin / P.M;
+    qN = (P.Qc / P.M - 0.3f) * (1.f / 0.3f);
+    rN = (std::log(r) - 1.7917595f) * (2.f / 2.3025851f) - 1.f;
+    iN = (incl - 45.f) * (1.f / 43.f);
+}
+
+}  // namespace
+
+struct BHSurrogate
+{
+    SgState S;
+    cudaStream_t stream = nullptr;
+    // frame scratch
+    unsigned* list = nullptr;
+    size_t listCap = 0;
+    unsigned* counters = nullptr;     // [0] RK4 list size, [1] held-out count, [4..7] held-out statistics
+    unsigned* heldPix = nullptr;
+    float4* heldPred = nullptr;
+    unsigned heldCap = 0;
+    unsigned frames = 0;
+    unsigned lastPixels = 0;
+    // critical curve cache
+    bool critValid = false;
+    CritKey critKey;
+    float crit[kCritBins];
+    // batch buffers of the training loop
+    float* bIn = nullptr;
+    float* bTgt = nullptr;
+    int bCap = 0;
+};
+
+namespace {
+
+void freeAll(BHSurrogate* s)
+{
+    SgState& S = s->S;
+    sg_free_batch(S);
+    void* ps[] = {S.params, S.grads, S.adamM, S.adamV, S.W, S.Wt, S.biasPacked, S.loss, S.dsIn, S.dsTgt, s->list,
+                  s->counters, s->heldPix, s->heldPred, s->bIn, s->bTgt};
+    for (void* p : ps)
+        if (p) cudaFree(p);
+    if (s->stream) cudaStreamDestroy(s->stream);
+    delete s;
+}
+
+cudaError_t checkErrWord(BHSurrogate* s)
+{
+    unsigned flags = 0;
+    cudaError_t e = cudaMemcpy(&flags, s->S.err, sizeof(unsigned), cudaMemcpyDeviceToHost);
+    if (e != cudaSuccess) return e;
+    if (flags)
+    {
+        unsigned zero = 0;
+        cudaMemcpy(s->S.err, &zero, sizeof(unsigned), cudaMemcpyHostToDevice);
+        return cudaErrorTimeout;
+    }
+    return cudaSuccess;
+}
+
+// Critical screen radius (tan units) per polar angle: bisection between a ray
+// aimed at the hole (captured) and one far outside (escaped), FP32 RK4 without
+// the disk, all angle bins in one probe launch per step.
+cudaError_t criticalCurve(BHSurrogate* s, const RenderParams& P0, float* crit)
+{
+    RenderParams P = P0;
+    P.diskEnabled = 0;
+    P.hotSpotsEnabled = 0;
+    const int n = kCritBins;
+    std::vector<float> lo(n, 0.f), hi(n, 4.f);
+    std::vector<float3> dirs(n);
+    std::vector<BHProbe> rec(n);
+    float3* dDirs = nullptr;
+    BHProbe* dRec = nullptr;
+    cudaError_t e = cudaMalloc(&dDirs, n * sizeof(float3));
+    if (e == cudaSuccess) e = cudaMalloc(&dRec, n * sizeof(BHProbe));
+    auto dirFor = [&](int k, float rho) {
+        const float psi = 2.f * kPi * (float)k / (float)n;
+        const float sx = rho * std::cos(psi), sy = rho * std::sin(psi);
+        float3 d{P.camForward.x + P.camRight.x * sx + P.camUp.x * sy,
+                 P.camForward.y + P.camRight.y * sx + P.camUp.y * sy,
+                 P.camForward.z + P.camRight.z * sx + P.camUp.z * sy};
+        const float l = length3(d);
+        return float3{d.x / l, d.y / l, d.z / l};
+    };
+    for (int it = 0; it < 22 && e == cudaSuccess; ++it)
+    {
+        for (int k = 0; k < n; ++k) dirs[k] = dirFor(k, 0.5f * (lo[k] + hi[k]));
+        e = cudaMemcpyAsync(dDirs, dirs.data(), n * sizeof(float3), cudaMemcpyHostToDevice, s->stream);
+        if (e == cudaSuccess) e = bhProbeRays(dRec, dDirs, n, P, BH_PREC_FP32, s->stream);
+        if (e == cudaSuccess)
+            e = cudaMemcpyAsync(rec.data(), dRec, n * sizeof(BHProbe), cudaMemcpyDeviceToHost, s->stream);
+        if (e == cudaSuccess) e = cudaStreamSynchronize(s->stream);
+        for (int k = 0; k < n && e == cudaSuccess; ++k)
+        {
+            const float mid = 0.5f * (lo[k] + hi[k]);
+            if (rec[k].outcome == 1) hi[k] = mid; else lo[k] = mid;
+        }
+    }
+    for (int k = 0; k < n; ++k) crit[k] = 0.5f * (lo[k] + hi[k]);
+    if (dDirs) cudaFree(dDirs);
+    if (dRec) cudaFree(dRec);
+    return e;
+}
+
+cudaError_t ensureFrame(BHSurrogate* s, size_t pixels)
+{
+    if (pixels <= s->listCap) return cudaSuccess;
+    if (s->list) cudaFree(s->list);
+    if (s->heldPix) cudaFree(s->heldPix);
+    if (s->heldPred) cudaFree(s->heldPred);
+    s->list = nullptr; s->heldPix = nullptr; s->heldPred = nullptr; s->listCap = 0; s->heldCap = 0;
+    const unsigned cap = (unsigned)(pixels / kHeldStride * 2 + 4096);
+    cudaError_t e = cudaMalloc(&s->list, pixels * sizeof(unsigned));
+    if (e == cudaSuccess) e = cudaMalloc(&s->heldPix, cap * sizeof(unsigned));
+    if (e == cudaSuccess) e = cudaMalloc(&s->heldPred, cap * sizeof(float4));
+    if (e != cudaSuccess) return e;
+    s->listCap = pixels;
+    s->heldCap = cap;
+    return cudaSuccess;
+}
+
+}  // namespace
+
+extern "C" {
+
+int bhSurrogateParamCount(void) { return SgLayout::count(); }
+
+cudaError_t bhSurrogateCreate(BHSurrogate** out, unsigned seed)
+{
+    if (!out) return cudaErrorInvalidValue;
+    *out = nullptr;
+    BHSurrogate* s = new BHSurrogate();
+    SgState& S = s->S;
+    const size_t pc = (size_t)SgLayout::count() * sizeof(float);
+    cudaError_t e = cudaGetDevice(&S.device);
+    if (e == cudaSuccess) e = cudaStreamCreateWithFlags(&s->stream, cudaStreamNonBlocking);
+    if (e == cudaSuccess) e = cudaMalloc(&S.params, pc);
+    if (e == cudaSuccess) e = cudaMalloc(&S.grads, pc);
+    if (e == cudaSuccess) e = cudaMalloc(&S.adamM, pc);
+    if (e == cudaSuccess) e = cudaMalloc(&S.adamV, pc);
+    if (e == cudaSuccess) e = cudaMalloc(&S.W, kWCount * 2);
+    if (e == cudaSuccess) e = cudaMalloc(&S.Wt, kWCount * 2);
+    if (e == cudaSuccess) e = cudaMalloc(&S.biasPacked, kBiasCount * sizeof(float));
+    if (e == cudaSuccess) e = cudaMalloc(&S.loss, 8 * sizeof(float));
+    if (e == cudaSuccess) e = cudaMalloc(&s->counters, 64);
+    if (e == cudaSuccess) e = bh_tc_error_word(&S.err);
+    if (e == cudaSuccess) e = cudaMemset(S.W, 0, kWCount * 2);
+    if (e != cudaSuccess) { freeAll(s); return e; }
+    // Xavier-uniform weights, zero biases
+    std::vector<float> p(SgLayout::count(), 0.f);
+    std::mt19937 g(seed);
+    for (int l = 0; l < 4; ++l)
+    {
+        const float lim = std::sqrt(6.f / 512.f);
+        for (int i = 0; i < kHidW; ++i) p[SgLayout::w(l) + i] = uni(g, -lim, lim);
+    }
+    const float limH = std::sqrt(6.f / (256.f + 16.f));
+    for (int i = 0; i < 16 * 256; ++i) p[SgLayout::w(4) + i] = uni(g, -limH, limH);
+    *out = s;
+    e = bhSurrogateSetParams(s, p.data());
+    if (e != cudaSuccess) { freeAll(s); *out = nullptr; }
+    return e;
+}
+
+void bhSurrogateDestroy(BHSurrogate* s)
+{
+    if (!s) return;
+    cudaStreamSynchronize(s->stream);
+    freeAll(s);
+}
+
+cudaError_t bhSurrogateGetParams(BHSurrogate* s, float* host)
+{
+    if (!s || !host) return cudaErrorInvalidValue;
+    cudaError_t e = cudaStreamSynchronize(s->stream);
+    if (e != cudaSuccess) return e;
+    return cudaMemcpy(host, s->S.params, SgLayout::count() * sizeof(float), cudaMemcpyDeviceToHost);
+}
+
+cudaError_t bhSurrogateSetParams(BHSurrogate* s, const float* host)
+{
+    if (!s || !host) return cudaErrorInvalidValue;
+    SgState& S = s->S;
+    const size_t pc = (size_t)SgLayout::count() * sizeof(float);
+    cudaError_t e = cudaStreamSynchronize(s->stream);
+    if (e == cudaSuccess) e = cudaMemcpy(S.params, host, pc, cudaMemcpyHostToDevice);
+    if (e == cudaSuccess) e = cudaMemset(S.adamM, 0, pc);
+    if (e == cudaSuccess) e = cudaMemset(S.adamV, 0, pc);
+    if (e == cudaSuccess) e = sg_pack_weights(S, s->stream);
+    if (e == cudaSuccess) e = cudaStreamSynchronize(s->stream);
+    S.step = 0;
+    return e;
+}
+
+cudaError_t bhSurrogateFeatures(const float* in, void* features, int n, cudaStream_t stream)
+{
+    if (n < 0 || (n > 0 && (!in || !features))) return cudaErrorInvalidValue;
+    return sg_features(in, features, n, stream);
+}
+
+cudaError_t bhSurrogateForward(BHSurrogate* s, const float* in, float* out, int n, int fused, cudaStream_t stream)
+{
+    if (!s || n < 0 || (n > 0 && (!in || !out))) return cudaErrorInvalidValue;
+    if (n == 0) return cudaSuccess;
+    SgState& S = s->S;
+    if (fused)
+    {
+        SgInferArgs a{S.W, S.W + 4 * kHidW, S.biasPacked, in, out, (unsigned)n, S.err};
+        return sg_infer_launch(a, nullptr, stream);
+    }
+    cudaError_t e = sg_forward_train(S, in, n, stream);
+    if (e != cudaSuccess) return e;
+    return cudaMemcpyAsync(out, S.Y, (size_t)n * 16 * sizeof(float), cudaMemcpyDeviceToDevice, stream);
+}
+
+cudaError_t bhSurrogateGradients(BHSurrogate* s, const float* in, const float* tgt, int n, float* gradsHost,
+                                 float* lossHost)
+{
+    if (!s || !in || !tgt || n <= 0 || n % 128) return cudaErrorInvalidValue;
+    SgState& S = s->S;
+    cudaError_t e = sg_gradients(S, in, tgt, n, s->stream);
+    if (e == cudaSuccess) e = cudaStreamSynchronize(s->stream);
+    if (e == cudaSuccess) e = checkErrWord(s);
+    if (e == cudaSuccess && gradsHost)
+        e = cudaMemcpy(gradsHost, S.grads, SgLayout::count() * sizeof(float), cudaMemcpyDeviceToHost);
+    if (e == cudaSuccess && lossHost)
+    {
+        float l[8];
+        e = cudaMemcpy(l, S.loss, sizeof(l), cudaMemcpyDeviceToHost);
+        for (int k = 0; k < 5; ++k) lossHost[k] = l[k] / (float)n;
+    }
+    return e;
+}
+
+cudaError_t bhSurrogateGenerate(BHSurrogate* s, long long rays, int views, unsigned seed)
+{
+    if (!s || rays <= 0 || views <= 0 || rays % views) return cudaErrorInvalidValue;
+    SgState& S = s->S;
+    const long long R = rays / views;
+    if (R > (1 << 26)) return cudaErrorInvalidValue;
+    cudaError_t e = cudaStreamSynchronize(s->stream);
+    if (S.dsN != rays)
+    {
+        if (S.dsIn) cudaFree(S.dsIn);
+        if (S.dsTgt) cudaFree(S.dsTgt);
+        S.dsIn = S.dsTgt = nullptr;
+        S.dsN = 0;
+        if (e == cudaSuccess) e = cudaMalloc(&S.dsIn, (size_t)rays * 8 * sizeof(float));
+        if (e == cudaSuccess) e = cudaMalloc(&S.dsTgt, (size_t)rays * 8 * sizeof(float));
+        if (e != cudaSuccess) return e;
+    }
+    float3* dirs = nullptr;
+    BHProbe* rec = nullptr;
+    if (e == cudaSuccess) e = cudaMalloc(&dirs, (size_t)R * sizeof(float3));
+    if (e == cudaSuccess) e = cudaMalloc(&rec, (size_t)R * sizeof(BHProbe));
+    std::mt19937 g(seed);
+    for (int v = 0; v < views && e == cudaSuccess; ++v)
+    {
+        const int model = (int)(g() % 4u);
+        float a = 0.f, q = 0.f;
+        do { a = uni(g, -0.998f, 0.998f); q = uni(g, 0.f, 0.6f); } while (a * a + q * q > 0.98f);
+        if (model == BH_SCHWARZSCHILD || model == BH_REISSNER_NORDSTROM) a = 0.f;
+        if (model == BH_SCHWARZSCHILD || model == BH_KERR) q = 0.f;
+        const float r = uni(g, 6.f, 60.f), incl = uni(g, 2.f, 88.f), az = uni(g, 0.f, 2.f * kPi);
+        const float fov = uni(g, 30.f, 90.f);
+        RenderParams P;
+        P.width = 1920; P.height = 1080;
+        applyHole(P, model, a, q);
+        orbitCamera(P, az, (90.f - incl) * kPi / 180.f, r, fov);
+        P.diskEnabled = 1; P.hotSpotsEnabled = (g() & 1u) ? 1 : 0;
+        P.dPhi = 0.012f; P.maxSteps = 2000;
+        P.accumMode = 0; P.sampleIndex = 0;
+        bhSanitizeRenderParams(&P);
+        float aN, qN, rN, iN;
+        sceneInputs(P, aN, qN, rN, iN);
+        const TraceParams tp = bh_frame_params(P, BH_OUT_PROBE, nullptr);
+        float* in = S.dsIn + (size_t)v * R * 8;
+        float* tgt = S.dsTgt + (size_t)v * R * 8;
+        e = sg_make_rays(tp, aN, qN, rN, iN, seed * 0x9E3779B1u + (unsigned)v * 0x85EBCA77u, dirs, in, (int)R,
+                         s->stream);
+        if (e == cudaSuccess) e = bhProbeRays(rec, dirs, (int)R, P, BH_PREC_FP32, s->stream);
+        if (e == cudaSuccess) e = sg_make_targets(rec, tp, tgt, (int)R, s->stream);
+    }
+    if (e == cudaSuccess) e = cudaStreamSynchronize(s->stream);
+    if (dirs) cudaFree(dirs);
+    if (rec) cudaFree(rec);
+    if (e == cudaSuccess) S.dsN = rays;
+    return e;
+}
+
+cudaError_t bhSurrogateDataset(BHSurrogate* s, const float** in, const float** tgt, long long* n)
+{
+    if (!s) return cudaErrorInvalidValue;
+    if (in) *in = s->S.dsIn;
+    if (tgt) *tgt = s->S.dsTgt;
+    if (n) *n = s->S.dsN;
+    return cudaSuccess;
+}
+
+cudaError_t bhSurrogateTrain(BHSurrogate* s, int steps, int batch, float lr, unsigned seed, float* lossHistory)
+{
+    if (!s || steps < 0 || batch <= 0 || batch % 128 || !(lr > 0.f)) return cudaErrorInvalidValue;
+    SgState& S = s->S;
+    if (S.dsN <= 0) return cudaErrorInvalidValue;
+    cudaError_t e = cudaSuccess;
+    if (batch > s->bCap)
+    {
+        if (s->bIn) cudaFree(s->bIn);
+        if (s->bTgt) cudaFree(s->bTgt);
+        s->bIn = s->bTgt = nullptr;
+        s->bCap = 0;
+        if ((e = cudaMalloc(&s->bIn, (size_t)batch * 8 * sizeof(float))) != cudaSuccess) return e;
+        if ((e = cudaMalloc(&s->bTgt, (size_t)batch * 8 * sizeof(float))) != cudaSuccess) return e;
+        s->bCap = batch;
+    }
+    float* hist = nullptr;
+    if (steps > 0 && (e = cudaMalloc(&hist, (size_t)steps * 8 * sizeof(float))) != cudaSuccess) return e;
+    for (int it = 0; it < steps && e == cudaSuccess; ++it)
+    {
+        const float t = steps > 1 ? (float)it / (float)(steps - 1) : 0.f;
+        const float lrT = lr * (0.05f + 0.95f * 0.5f * (1.f + std::cos(kPi * t)));
+        e = sg_gather(S, seed * 0x9E3779B1u + (unsigned)it * 0x632BE5ABu, s->bIn, s->bTgt, batch, s->stream);
+        if (e == cudaSuccess) e = sg_gradients(S, s->bIn, s->bTgt, batch, s->stream);
+        if (e == cudaSuccess) e = sg_adam(S, lrT, s->stream);
+        if (e == cudaSuccess)
+            e = cudaMemcpyAsync(hist + (size_t)it * 8, S.loss, 8 * sizeof(float), cudaMemcpyDeviceToDevice, s->stream);
+    }
+    if (e == cudaSuccess) e = cudaStreamSynchronize(s->stream);
+    if (e == cudaSuccess) e = checkErrWord(s);
+    if (e == cudaSuccess && lossHistory && steps > 0)
+    {
+        std::vector<float> h((size_t)steps * 8);
+        e = cudaMemcpy(h.data(), hist, h.size() * sizeof(float), cudaMemcpyDeviceToHost);
+        for (int it = 0; it < steps; ++it)
+            for (int k = 0; k < 5; ++k) lossHistory[it * 5 + k] = h[(size_t)it * 8 + k] / (float)batch;
+    }
+    if (hist) cudaFree(hist);
+    return e;
+}
+
+cudaError_t bhSurrogateRender(BHSurrogate* s, uchar4* out, float4* accum, float4* bloomA, float4* bloomB,
+                              const RenderParams* p, cudaStream_t stream)
+{
+    if (!s || !p) return cudaErrorInvalidValue;
+    RenderParams P = *p;
+    bhSanitizeRenderParams(&P);
+    if (!out || !accum || (P.bloomEnabled && (!bloomA || !bloomB))) return cudaErrorInvalidValue;
+    if (std::fabs(P.camRight.y) > 1e-4f || P.accumMode != 0) return cudaErrorInvalidValue;
+    const size_t pixels = (size_t)P.width * P.height;
+    cudaError_t e = ensureFrame(s, pixels);
+    if (e != cudaSuccess) return e;
+    CritKey key;
+    key.model = P.model; key.maxSteps = P.maxSteps; key.M = P.M; key.a = P.aSpin; key.Q = P.Qc;
+    key.dist = length3(P.camPos); key.cosIncl = P.camPos.y / key.dist; key.tanHalfFov = P.tanHalfFov;
+    key.dPhi = P.dPhi;
+    if (!s->critValid || !(key == s->critKey))
+    {
+        if ((e = criticalCurve(s, P, s->crit)) != cudaSuccess) return e;
+        s->critKey = key;
+        s->critValid = true;
+    }
+    SgState& S = s->S;
+    SgFrame F{};
+    F.tp = bh_frame_params(P, BH_OUT_ACCUM, accum);
+    sceneInputs(P, F.aN, F.qN, F.rN, F.iN);
+    std::memcpy(F.crit, s->crit, sizeof(F.crit));
+    F.critBand = 0.02f;
+    F.minProb = 0.95f;
+    F.minConf = 0.95f;
+    F.list = s->list;
+    F.listCount = s->counters;
+    F.heldPix = s->heldPix;
+    F.heldPred = s->heldPred;
+    F.heldCount = s->counters + 1;
+    F.heldCap = s->heldCap;
+    F.heldStride = kHeldStride;
+    F.frameSeed = ++s->frames;
+    s->lastPixels = (unsigned)pixels;
+    if ((e = cudaMemsetAsync(s->counters, 0, 64, stream)) != cudaSuccess) return e;
+    SgInferArgs a{S.W, S.W + 4 * kHidW, S.biasPacked, nullptr, nullptr, (unsigned)pixels, S.err};
+    if ((e = sg_infer_launch(a, &F, stream)) != cudaSuccess) return e;
+    // RK4 for the listed pixels
+    TraceParams t = F.tp;
+    t.pixList = s->list;
+    t.nRaysDev = s->counters;
+    t.nRays = (unsigned)pixels;
+    if ((e = bh_device_counter(&t.counter)) != cudaSuccess) return e;
+    if ((e = bh_launch_trace(t, BH_PREC_FP32, false, bh_family_blocks(P), stream)) != cudaSuccess) return e;
+    if ((e = sg_held_compare(accum, s->heldPix, s->heldPred, s->counters + 1, s->heldCap, F.tp, s->counters + 4,
+                             stream)) != cudaSuccess)
+        return e;
+    PostConsts pc{P.exposure, P.bloomStrength, P.bloomEnabled ? 1 : 0, P.swapRB};
+    return bh_launch_post(out, accum, bloomB, P.width, P.height, pc, stream);
+}
+
+cudaError_t bhSurrogateFrameStats(BHSurrogate* s, BHSurrogateStats* st)
+{
+    if (!s || !st) return cudaErrorInvalidValue;
+    unsigned c[16];
+    cudaError_t e = cudaDeviceSynchronize();
+    if (e == cudaSuccess) e = cudaMemcpy(c, s->counters, sizeof(c), cudaMemcpyDeviceToHost);
+    if (e == cudaSuccess) e = checkErrWord(s);
+    if (e != cudaSuccess) return e;
+    st->pixels = s->lastPixels;
+    st->rk4Pixels = c[0];
+    st->heldOut = c[4];
+    st->heldOutOver1Lsb = c[5];
+    float mx;
+    std::memcpy(&mx, &c[6], sizeof(float));
+    st->heldOutMaxAbs = mx;
+    st->heldOutOverTol = c[7];
+    return cudaSuccess;
+}
+
+}  // extern "C"
+
+extern "C" cudaError_t bhSurrogateDatasetCopy(BHSurrogate* s, float* in, float* tgt, long long first, long long count)
+{
+    if (!s || first < 0 || count < 0 || first + count > s->S.dsN) return cudaErrorInvalidValue;
+    cudaError_t e = cudaStreamSynchronize(s->stream);
+    if (e == cudaSuccess && in)
+        e = cudaMemcpy(in, s->S.dsIn + first * 8, (size_t)count * 8 * sizeof(float), cudaMemcpyDeviceToHost);
+    if (e == cudaSuccess && tgt)
+        e = cudaMemcpy(tgt, s->S.dsTgt + first * 8, (size_t)count * 8 * sizeof(float), cudaMemcpyDeviceToHost);
+    return e;
+}

@@ -1,0 +1,416 @@
+// ---------------------------------------------------------------------------
+// bh_sg_infer.cu -- fused, persistent inference of the lensing surrogate on
+// the tensor cores: Fourier features -> 4 x (256 x 256 GEMM + GELU) -> head,
+// one launch, activations never leave shared memory.
+//
+// CTA = 10 warps, one per SM (shared memory ~198 KB, all 512 TMEM columns):
+//   warps 0-3  epilogue group 0: 128 rays (one per thread) of tile A0
+//   warps 4-7  epilogue group 1: 128 rays of tile A1
+//   warp 8     TMA producer: streams 128 x 64 weight chunks (16 KB) through a
+//              4-stage ring (the 4 hidden layers are one 1024 x 256 tensor)
+//   warp 9     MMA issuer: tcgen05.mma M=128 N=128 K=16, accumulators in TMEM
+//              (group g owns columns 256g .. 256g + 255)
+// The two groups ping-pong: while group 0 turns layer l's accumulator into
+// layer l+1's BF16 operand (bias, GELU, 128-byte-swizzled stores), the tensor
+// core runs layer l of group 1, and the other way round.  Per tile pair the
+// producer and the issuer walk the same chunk sequence:
+//   for l in 0..3: for g in 0..1: for kb in 0..3: for half in 0..1: W_l[half rows, kb cols]
+//   then for g in 0..1: for kb in 0..3: W_head[:, kb cols]
+// Barriers: full/empty per ring stage, aReady[g] (128 epilogue arrivals: the
+// operand of the next layer is in shared memory and the accumulator is free),
+// accFull[g] (MMA commit: layer done).  All waits are bounded (bh_tc.cuh).
+// ---------------------------------------------------------------------------
+#include <cuda.h>
+#include <cuda_bf16.h>
+#include "bh_integrate.cuh"
+#include "bh_post.cuh"
+#include "bh_sg_infer.h"
+#include "bh_sg_net.cuh"
+#include "bh_tc.cuh"
+
+using namespace bhtc;
+using namespace bhsg;
+
+namespace {
+
+constexpr int kRing = 4;
+constexpr uint32_t kTileBytes = 128u * 256u * 2u;       // one group's operand: 128 rows x 256 BF16
+constexpr uint32_t kChunkBytes = 128u * 128u;           // 128 weight rows x 64 BF16
+constexpr uint32_t kHeadChunkBytes = 16u * 128u;        // 16 head rows x 64 BF16
+constexpr int kThreads = 320;
+constexpr uint32_t kSmemBytes = 2 * kTileBytes + kRing * kChunkBytes + 1024;
+
+struct Bars
+{
+    uint64_t full[kRing], empty[kRing], aReady[2], accFull[2];
+    uint32_t tmem;
+};
+
+// 8 packed BF16 values -> the operand row `row`, columns col .. col + 7
+__device__ __forceinline__ void st_chunk(uint8_t* tile, uint32_t row, uint32_t col, uint4 v)
+{
+    *reinterpret_cast<uint4*>(tile + sw128_offset(row, col, 128)) = v;
+}
+
+__device__ __forceinline__ uint32_t pack_gelu(float a, float b)
+{
+    __nv_bfloat162 h = gelu2(__floats2bfloat162_rn(a, b));
+    return *reinterpret_cast<uint32_t*>(&h);
+}
+
+// Network inputs of one ray.
+struct RayIn
+{
+    float x[kIn];
+    f3 dirW;          // world direction (frame mode)
+};
+
+__device__ __forceinline__ void frame_inputs(const SgFrame& F, unsigned pix, RayIn& r)
+{
+    const TraceParams& P = F.tp;
+    const int py = (int)(pix / (unsigned)P.W), px = (int)(pix - (unsigned)py * (unsigned)P.W);
+    const float fx = __fdiv_rn(add_x((float)px, P.jx), (float)P.W);
+    const float fy = __fdiv_rn(add_x((float)py, P.jy), (float)P.H);
+    const f3 d = camera_ray(P, fx, fy);
+    r.dirW = d;
+    r.x[0] = d.x * P.camRight.x + d.y * P.camRight.y + d.z * P.camRight.z;
+    r.x[1] = d.x * P.camUp.x + d.y * P.camUp.y + d.z * P.camUp.z;
+    r.x[2] = d.x * P.camFwd.x + d.y * P.camFwd.y + d.z * P.camFwd.z;
+    r.x[3] = F.aN; r.x[4] = F.qN; r.x[5] = F.rN; r.x[6] = F.iN;
+}
+
+// Is the pixel within the critical band (|rho / rho_c(psi) - 1| < band)?
+__device__ __forceinline__ bool near_critical(const SgFrame& F, float cx, float cy)
+{
+    const float rho = sqrtf(cx * cx + cy * cy);
+    float psi = atan2f(cy, cx) * (0.159154943f * (float)kCritBins);
+    if (psi < 0.f) psi += (float)kCritBins;
+    int b0 = (int)psi;
+    const float t = psi - (float)b0;
+    b0 = min(b0, kCritBins - 1);
+    const int b1 = (b0 + 1) % kCritBins;
+    const float rc = F.crit[b0] * (1.f - t) + F.crit[b1] * t;
+    return fabsf(rho - rc) < F.critBand * rc;
+}
+
+// Per-ray decision after the head: shade from the surrogate or queue for RK4.
+__device__ void frame_output(const SgFrame& F, unsigned pix, bool valid, const RayIn& r, const float* y)
+{
+    bool fallback = false, held = false;
+    f3 hdr = v3(0.f, 0.f, 0.f);
+    if (valid)
+    {
+        const float m = fmaxf(y[0], fmaxf(y[1], y[2]));
+        const float e0 = __expf(y[0] - m), e1 = __expf(y[1] - m), e2 = __expf(y[2] - m);
+        const float inv = 1.f / (e0 + e1 + e2);
+        const float p0 = e0 * inv, p1 = e1 * inv;
+        const int cls = (p0 >= p1 && p0 >= e2 * inv) ? kClsEscaped : (p1 >= e2 * inv ? kClsCaptured : kClsDisk);
+        const float pc = cls == kClsEscaped ? p0 : (cls == kClsCaptured ? p1 : e2 * inv);
+        const float conf = 1.f / (1.f + __expf(-y[kOConf]));
+        // screen-plane position of the ray (tan-space, camera basis)
+        const float cx = r.x[0] / r.x[2], cy = r.x[1] / r.x[2];
+        fallback = cls == kClsDisk || pc < F.minProb || conf < F.minConf || near_critical(F, cx, cy);
+        if (!fallback)
+        {
+            if (cls == kClsEscaped)
+            {
+                f3 e = v3(r.x[0] + y[kOEsc], r.x[1] + y[kOEsc + 1], r.x[2] + y[kOEsc + 2]);
+                const TraceParams& P = F.tp;
+                f3 w = v3(P.camRight.x * e.x + P.camUp.x * e.y + P.camFwd.x * e.z,
+                          P.camRight.y * e.x + P.camUp.y * e.y + P.camFwd.y * e.z,
+                          P.camRight.z * e.x + P.camUp.z * e.y + P.camFwd.z * e.z);
+                hdr = sky_color(w, P.gCam);
+                if (!isfinite(hdr.x) || !isfinite(hdr.y) || !isfinite(hdr.z)) hdr = v3(0.f, 0.f, 0.f);
+            }
+            // held-out check: every heldStride-th surrogate pixel (hashed per frame) is also traced
+            unsigned h = pix * 0x9E3779B1u ^ (F.frameSeed * 0x85EBCA77u);
+            h ^= h >> 15; h *= 0x2C1B3C6Du; h ^= h >> 12;
+            held = F.heldStride > 0 && (h % (unsigned)F.heldStride) == 0u;
+            float4* acc = reinterpret_cast<float4*>(F.tp.out);
+            acc[pix] = make_float4(hdr.x, hdr.y, hdr.z, 1.f);
+        }
+    }
+    // warp-aggregated appends to the RK4 list (fallback and held-out pixels)
+    const unsigned lane = threadIdx.x & 31u;
+    const bool push = fallback || held;
+    const unsigned m = __ballot_sync(0xffffffffu, push);
+    if (m)
+    {
+        unsigned base = 0;
+        if (lane == (unsigned)(__ffs(m) - 1)) base = atomicAdd(F.listCount, (unsigned)__popc(m));
+        base = __shfl_sync(0xffffffffu, base, __ffs(m) - 1);
+        if (push) F.list[base + __popc(m & ((1u << lane) - 1u))] = pix;
+    }
+    const unsigned mh = __ballot_sync(0xffffffffu, held);
+    if (mh)
+    {
+        unsigned base = 0;
+        if (lane == (unsigned)(__ffs(mh) - 1)) base = atomicAdd(F.heldCount, (unsigned)__popc(mh));
+        base = __shfl_sync(0xffffffffu, base, __ffs(mh) - 1);
+        if (held)
+        {
+            const unsigned k = base + __popc(mh & ((1u << lane) - 1u));
+            if (k < F.heldCap)
+            {
+                F.heldPix[k] = pix;
+                F.heldPred[k] = make_float4(hdr.x, hdr.y, hdr.z, 1.f);
+            }
+        }
+    }
+}
+
+template <bool FRAME>
+__global__ void __launch_bounds__(kThreads, 1)
+sg_infer_kernel(const __grid_constant__ CUtensorMap tW, const __grid_constant__ CUtensorMap tH,
+                const __grid_constant__ SgFrame F, const float* __restrict__ bias, const float* __restrict__ rawIn,
+                float* __restrict__ rawOut, unsigned n, unsigned iters, unsigned* __restrict__ err)
+{
+    extern __shared__ uint8_t smemRaw[];
+    __shared__ Bars B;
+    __shared__ float sBias[kHidden * kWidth + kOut];
+    uint8_t* smem = reinterpret_cast<uint8_t*>((reinterpret_cast<uintptr_t>(smemRaw) + 1023) & ~uintptr_t(1023));
+    uint8_t* tiles = smem;                       // 2 x 64 KB operands
+    uint8_t* ring = smem + 2 * kTileBytes;       // 4 x 16 KB weight chunks
+    const int warp = threadIdx.x >> 5, lane = threadIdx.x & 31;
+
+    for (int i = threadIdx.x; i < kHidden * kWidth + kOut; i += kThreads) sBias[i] = bias[i];
+    if (threadIdx.x == 0)
+    {
+        for (int s = 0; s < kRing; ++s) { mbar_init(&B.full[s], 1); mbar_init(&B.empty[s], 1); }
+        for (int g = 0; g < 2; ++g) { mbar_init(&B.aReady[g], 128); mbar_init(&B.accFull[g], 1); }
+        fence_barrier_init();
+    }
+    if (warp == 8)
+    {
+        __syncwarp();
+        tmem_alloc(&B.tmem, 512);
+    }
+    tc_fence_before();
+    __syncthreads();
+    tc_fence_after();
+    const uint32_t tmem = B.tmem;
+
+    if (warp == 8)
+    {
+        if (lane == 0)
+        {   // ---- TMA producer ----
+            tma_prefetch_desc(&tW);
+            tma_prefetch_desc(&tH);
+            uint32_t q = 0;
+            bool ok = true;
+            for (unsigned it = 0; it < iters && ok; ++it)
+            {
+                for (int l = 0; l <= kHidden && ok; ++l)
+                    for (int g = 0; g < 2 && ok; ++g)
+                        for (int kb = 0; kb < 4 && ok; ++kb)
+                            for (int h = 0; h < (l < kHidden ? 2 : 1) && ok; ++h, ++q)
+                            {
+                                const uint32_t s = q % kRing;
+                                if (q >= kRing && !(ok = mbar_wait(&B.empty[s], ((q / kRing) - 1) & 1, err))) break;
+                                uint8_t* dst = ring + s * kChunkBytes;
+                                if (l < kHidden)
+                                {
+                                    mbar_expect_tx(&B.full[s], kChunkBytes);
+                                    tma_load_2d(dst, &tW, &B.full[s], kb * 64, l * 256 + h * 128);
+                                }
+                                else
+                                {
+                                    mbar_expect_tx(&B.full[s], kHeadChunkBytes);
+                                    tma_load_2d(dst, &tH, &B.full[s], kb * 64, 0);
+                                }
+                            }
+            }
+            // drain: the last loads must land before the CTA may exit
+            if (ok && q > 0)
+                for (uint32_t k = (q > kRing ? q - kRing : 0); k < q; ++k)
+                    if (!mbar_wait(&B.full[k % kRing], (k / kRing) & 1, err)) break;
+        }
+    }
+    else if (warp == 9)
+    {
+        if (lane == 0)
+        {   // ---- MMA issuer ----
+            const uint32_t idH = idesc_bf16_f32(128), idHead = idesc_bf16_f32(kOut);
+            uint32_t q = 0, phA[2] = {0, 0};
+            bool ok = true;
+            for (unsigned it = 0; it < iters && ok; ++it)
+                for (int l = 0; l <= kHidden && ok; ++l)
+                    for (int g = 0; g < 2 && ok; ++g)
+                    {
+                        if (!(ok = mbar_wait(&B.aReady[g], phA[g], err))) break;
+                        phA[g] ^= 1u;
+                        tc_fence_after();
+                        const uint32_t aBase = smem_u32(tiles + g * kTileBytes);
+                        const uint32_t d = tmem + (uint32_t)g * 256u;
+                        for (int kb = 0; kb < 4 && ok; ++kb)
+                            for (int h = 0; h < (l < kHidden ? 2 : 1) && ok; ++h, ++q)
+                            {
+                                const uint32_t s = q % kRing;
+                                if (!(ok = mbar_wait(&B.full[s], (q / kRing) & 1, err))) break;
+                                tc_fence_after();
+                                const uint32_t bBase = smem_u32(ring + s * kChunkBytes);
+                                const uint32_t aBlk = aBase + (uint32_t)kb * 16384u;
+#pragma unroll
+                                for (int j = 0; j < 4; ++j)
+                                    mma_bf16(d + (uint32_t)h * 128u, sdesc_sw128(aBlk + j * 32), sdesc_sw128(bBase + j * 32),
+                                             l < kHidden ? idH : idHead, kb > 0 || j > 0);
+                                mma_commit(&B.empty[s]);
+                            }
+                        mma_commit(&B.accFull[g]);
+                    }
+        }
+    }
+    else
+    {   // ---- epilogue groups ----
+        const int g = warp >> 2, wq = warp & 3;
+        const uint32_t row = (uint32_t)(wq * 32 + lane);
+        uint8_t* tile = tiles + g * kTileBytes;
+        const uint32_t tl = tmem + (uint32_t)g * 256u + ((uint32_t)(wq * 32) << 16);
+        uint32_t phF = 0;
+        bool ok = true;
+        for (unsigned it = 0; it < iters && ok; ++it)
+        {
+            const unsigned tileIdx = (it * gridDim.x + blockIdx.x) * 2u + (unsigned)g;
+            const unsigned rid = tileIdx * 128u + row;
+            const bool valid = rid < n;
+            RayIn r;
+            if constexpr (FRAME)
+            {
+                frame_inputs(F, valid ? rid : 0u, r);
+            }
+            else
+            {
+#pragma unroll
+                for (int k = 0; k < kIn; ++k) r.x[k] = valid ? __ldg(rawIn + (size_t)rid * 8 + k) : 0.f;
+            }
+#pragma unroll 4
+            for (int j = 0; j < 32; ++j) st_chunk(tile, row, (uint32_t)j * 8u, sg_feature_chunk(r.x, j));
+            fence_async_smem();
+            mbar_arrive(&B.aReady[g]);
+
+            for (int l = 0; l < kHidden && ok; ++l)
+            {
+                ok = __all_sync(0xffffffffu, mbar_wait(&B.accFull[g], phF, err));
+                phF ^= 1u;
+                if (!ok) break;
+                tc_fence_after();
+                const float* bl = sBias + l * kWidth;
+#pragma unroll 1
+                for (int c = 0; c < kWidth; c += 32)
+                {
+                    float v[32];
+                    tmem_ld32(tl + (uint32_t)c, v);
+#pragma unroll
+                    for (int q4 = 0; q4 < 4; ++q4)
+                    {
+                        uint4 o;
+                        const int b = c + q4 * 8;
+                        o.x = pack_gelu(v[q4 * 8 + 0] + bl[b + 0], v[q4 * 8 + 1] + bl[b + 1]);
+                        o.y = pack_gelu(v[q4 * 8 + 2] + bl[b + 2], v[q4 * 8 + 3] + bl[b + 3]);
+                        o.z = pack_gelu(v[q4 * 8 + 4] + bl[b + 4], v[q4 * 8 + 5] + bl[b + 5]);
+                        o.w = pack_gelu(v[q4 * 8 + 6] + bl[b + 6], v[q4 * 8 + 7] + bl[b + 7]);
+                        st_chunk(tile, row, (uint32_t)b, o);
+                    }
+                }
+                tc_fence_before();
+                fence_async_smem();
+                mbar_arrive(&B.aReady[g]);
+            }
+            if (!ok) break;
+            ok = __all_sync(0xffffffffu, mbar_wait(&B.accFull[g], phF, err));
+            phF ^= 1u;
+            if (!ok) break;
+            tc_fence_after();
+            float y[kOut];
+            tmem_ld16(tl, y);
+            tc_fence_before();
+#pragma unroll
+            for (int k = 0; k < kOut; ++k) y[k] += sBias[kHidden * kWidth + k];
+            if constexpr (FRAME)
+            {
+                frame_output(F, rid, valid, r, y);
+            }
+            else if (valid)
+            {
+#pragma unroll
+                for (int k = 0; k < kOut; ++k) rawOut[(size_t)rid * kOut + k] = y[k];
+            }
+        }
+    }
+    tc_fence_before();
+    __syncthreads();
+    if (warp == 8)
+    {
+        __syncwarp();
+        tmem_free(tmem, 512);
+    }
+}
+
+}  // namespace
+
+cudaError_t sg_infer_launch(const SgInferArgs& a, const SgFrame* frame, cudaStream_t s)
+{
+    if (a.n == 0) return cudaSuccess;
+    CUtensorMap tW, tH;
+    cudaError_t e = bh_tensor_map_bf16(&tW, a.Whidden, kHidden * kWidth, kWidth, kWidth, 128);
+    if (e == cudaSuccess) e = bh_tensor_map_bf16(&tH, a.Whead, kOut, kWidth, kWidth, kOut);
+    if (e != cudaSuccess) return e;
+    int dev = 0, sms = 0;
+    if ((e = cudaGetDevice(&dev)) != cudaSuccess) return e;
+    if ((e = cudaDeviceGetAttribute(&sms, cudaDevAttrMultiProcessorCount, dev)) != cudaSuccess) return e;
+    const unsigned tiles = (a.n + 127u) / 128u;
+    const unsigned pairs = (tiles + 1u) / 2u;
+    const unsigned grid = std::min<unsigned>((unsigned)sms, pairs);
+    const unsigned iters = (pairs + grid - 1u) / grid;
+    SgFrame F{};
+    if (frame) F = *frame;
+    if (frame)
+    {
+        auto k = sg_infer_kernel<true>;
+        if ((e = cudaFuncSetAttribute(k, cudaFuncAttributeMaxDynamicSharedMemorySize, kSmemBytes))) return e;
+        k<<<grid, kThreads, kSmemBytes, s>>>(tW, tH, F, a.bias, nullptr, nullptr, a.n, iters, a.err);
+    }
+    else
+    {
+        auto k = sg_infer_kernel<false>;
+        if ((e = cudaFuncSetAttribute(k, cudaFuncAttributeMaxDynamicSharedMemorySize, kSmemBytes))) return e;
+        k<<<grid, kThreads, kSmemBytes, s>>>(tW, tH, F, a.bias, a.rawIn, a.rawOut, a.n, iters, a.err);
+    }
+    return cudaGetLastError();
+}
+
+namespace {
+
+__global__ void held_compare_kernel(const float4* __restrict__ accum, const unsigned* __restrict__ heldPix,
+                                    const float4* __restrict__ heldPred, const unsigned* __restrict__ heldCount,
+                                    unsigned heldCap, int W, float exposure, int swapRB, unsigned* __restrict__ stats)
+{
+    const unsigned k = blockIdx.x * blockDim.x + threadIdx.x;
+    const unsigned n = min(*heldCount, heldCap);
+    if (k >= n) return;
+    const unsigned pix = heldPix[k];
+    const int py = (int)(pix / (unsigned)W), px = (int)(pix - (unsigned)py * (unsigned)W);
+    const float4 a = accum[pix], b = heldPred[k];
+    const float d = fmaxf(fabsf(a.x - b.x), fmaxf(fabsf(a.y - b.y), fabsf(a.z - b.z)));
+    PostConsts pc{exposure, 0.f, 0, swapRB};
+    const uchar4 ua = finalize_pixel(v3(a.x, a.y, a.z), v3(0.f, 0.f, 0.f), pc, px, py);
+    const uchar4 ub = finalize_pixel(v3(b.x, b.y, b.z), v3(0.f, 0.f, 0.f), pc, px, py);
+    const int lsb = max(abs((int)ua.x - (int)ub.x), max(abs((int)ua.y - (int)ub.y), abs((int)ua.z - (int)ub.z)));
+    atomicAdd(stats + 0, 1u);
+    if (lsb > 1) atomicAdd(stats + 1, 1u);
+    atomicMax(stats + 2, __float_as_uint(d));
+    const float ref = fmaxf(fabsf(a.x), fmaxf(fabsf(a.y), fabsf(a.z)));
+    if (d > 1e-3f * fmaxf(ref, 1e-3f)) atomicAdd(stats + 3, 1u);
+}
+
+}  // namespace
+
+cudaError_t sg_held_compare(const float4* accum, const unsigned* heldPix, const float4* heldPred,
+                            const unsigned* heldCount, unsigned heldCap, const TraceParams& tp, unsigned* stats,
+                            cudaStream_t s)
+{
+    if (heldCap == 0) return cudaSuccess;
+    held_compare_kernel<<<(heldCap + 255) / 256, 256, 0, s>>>(accum, heldPix, heldPred, heldCount, heldCap, tp.W,
+                                                              tp.exposure, tp.swapRB, stats);
+    return cudaGetLastError();
+}

@@ -1,0 +1,53 @@
+// ---------------------------------------------------------------------------
+// bh_sg_infer.h -- launch interface of the fused surrogate inference kernel
+// (bh_sg_infer.cu) and of the per-frame held-out comparison.
+// ---------------------------------------------------------------------------
+#pragma once
+#include <cuda_runtime.h>
+#include "bh_surrogate.h"
+#include "bh_trace_params.h"
+
+constexpr int kCritBins = 512;
+
+// Frame mode: pixel k of the W x H frame is ray k.  Surrogate-resolved pixels
+// are written to the accumulation buffer (tp.out); RK4 pixels (disk class,
+// low probability or confidence, within critBand of the critical curve, and
+// the held-out sample) are appended to `list`.
+struct SgFrame
+{
+    TraceParams tp;
+    float aN, qN, rN, iN;           // normalised scene inputs
+    float crit[kCritBins];          // critical screen radius (tan units) per polar angle bin
+    float critBand;                 // relative half-width of the RK4 band around it
+    float minProb, minConf;         // class probability / confidence needed to keep a pixel
+    unsigned* list;                 // RK4 pixel list (capacity W * H)
+    unsigned* listCount;
+    unsigned* heldPix;              // held-out sample: pixel and surrogate HDR
+    float4* heldPred;
+    unsigned* heldCount;
+    unsigned heldCap;
+    int heldStride;                 // 1 in heldStride surrogate pixels is held out (0: none)
+    unsigned frameSeed;
+};
+
+struct SgInferArgs
+{
+    const void* Whidden;            // BF16 4 x 256 x 256 (out x in), stacked
+    const void* Whead;              // BF16 16 x 256
+    const float* bias;              // 4 x 256 + 16 (packed)
+    const float* rawIn;             // raw mode: n x 8 inputs
+    float* rawOut;                  // raw mode: n x 16 head outputs
+    unsigned n;                     // rays
+    unsigned* err;                  // device error word
+};
+
+// frame == nullptr: raw mode (rawIn -> rawOut)
+cudaError_t sg_infer_launch(const SgInferArgs& a, const SgFrame* frame, cudaStream_t s);
+
+// Held-out comparison after the RK4 pass: stats[0] += pixels compared,
+// stats[1] += pixels whose RGBA8 (exposure, no bloom) differs by more than
+// 1 LSB, stats[2] = max |HDR difference| (float bits), stats[3] += escaped
+// class disagreements (RK4 pixel not sky-only).
+cudaError_t sg_held_compare(const float4* accum, const unsigned* heldPix, const float4* heldPred,
+                            const unsigned* heldCount, unsigned heldCap, const TraceParams& tp, unsigned* stats,
+                            cudaStream_t s);

@@ -40,6 +40,13 @@ template <class R> struct Queue<R, true> { PackedRay<R> s[kWarps][kQueue]; Packe
 // ray id -> pixel (8x4 tiles, row-major tile order); false when outside the frame
 BH_DEV bool ray_pixel(const TraceParams& P, unsigned rid, int& px, int& py)
 {
+    if (P.pixList)
+    {
+        const unsigned pix = __ldg(P.pixList + rid);
+        py = (int)(pix / (unsigned)P.W);
+        px = (int)(pix - (unsigned)py * (unsigned)P.W);
+        return true;
+    }
     unsigned tile = rid >> 5, w = rid & 31u;
     if (P.tileOrder) tile = __ldg(P.tileOrder + tile);
     px = (int)((tile % (unsigned)P.tilesX) * 8u + (w & 7u));
@@ -142,6 +149,7 @@ trace_kernel(const __grid_constant__ TraceParams P)
     const unsigned FULL = 0xffffffffu, below = (1u << lane) - 1u;
     PackedRay<R>* ring = Q.s[warp];
 
+    const unsigned nRays = P.nRaysDev ? *P.nRaysDev : P.nRays;
     Ray ray;
     unsigned rid = 0, key = 0;
     bool live = false;
@@ -165,14 +173,14 @@ trace_kernel(const __grid_constant__ TraceParams P)
                 if (lane == 0) base = atomicAdd(P.counter, kChunk);
                 base = __shfl_sync(FULL, base, 0);
                 claimed = true;
-                if (base + kChunk >= P.nRays) drained = true;
+                if (base + kChunk >= nRays) drained = true;
             }
             if (!live)
             {
                 const unsigned rank = (unsigned)__popc(~liveMask & below);
                 unsigned id = (rank < avail) ? next + rank : base + (rank - avail);
-                bool valid = (rank < avail) || (claimed && base < P.nRays);
-                if (valid && id < P.nRays)
+                bool valid = (rank < avail) || (claimed && base < nRays);
+                if (valid && id < nRays)
                 {
                     int px = 0, py = 0;
                     bool inFrame = P.dirs ? true : ray_pixel(P, id, px, py);
@@ -187,9 +195,9 @@ trace_kernel(const __grid_constant__ TraceParams P)
                 }
             }
             if (avail >= nFree) next += nFree;
-            else if (claimed && base < P.nRays)
+            else if (claimed && base < nRays)
             {
-                end = min(base + kChunk, P.nRays);
+                end = min(base + kChunk, nRays);
                 next = min(base + (nFree - avail), end);
             }
             else next = end;

@@ -89,6 +89,8 @@ struct TraceParams
     unsigned* counter;            // ray counter, zeroed before the launch
     int refillMin;                // refill a warp when at least this many lanes are free
     const unsigned* tileOrder;    // non-null: k-th claimed tile -> tile index (trace order)
+    const unsigned* pixList;      // non-null: ray k traces pixel pixList[k] (y * W + x)
+    const unsigned* nRaysDev;     // non-null: the ray count is read here at kernel start
 
     CamFrame<float> cf;           // FP32 integration
     CamFrame<double> cd;          // FP64 integration

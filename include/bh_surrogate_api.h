@@ -37,6 +37,107 @@ cudaError_t bhTcGemm(const void* A, int lda, const void* B, int ldb, float* C, i
  * a bounded wait inside a kernel timed out (its results are invalid). */
 cudaError_t bhTcErrorFlags(unsigned* flags);
 
+/* ---- the network -------------------------------------------------------------
+ * Inputs, one row of 8 floats per ray: the unit ray direction in the camera
+ * basis (right, up, forward components), a* in [-1, 1], (q - 0.3) / 0.3,
+ * (ln r - ln 6) * 2 / ln 10 - 1 for camera distance r (code units), and
+ * (inclination - 45 deg) / 43 deg; the 8th float is ignored.
+ * Features: sin and cos of pi 2^(b/2) x for every input x and b = 0..15,
+ * plus the 7 inputs, zero-padded to 256 (BF16).
+ * Layers: 4 x (256 -> 256, tanh-form GELU), head 256 -> 16, BF16 weights and
+ * activations, FP32 accumulation.
+ * Head outputs (16 floats per ray): 0-2 class logits (0 escaped without
+ * touching the disk, 1 captured without touching the disk, 2 touched the
+ * disk); 3-5 added to the input direction give the camera-basis escape
+ * direction; 6 disk-hit radius / 8; 7 ln of the disk-hit redshift factor;
+ * 8 confidence logit; 9-15 unused.
+ * Targets, one row of 8 floats per ray: class, camera-basis unit escape
+ * direction (3), disk-hit radius / 8, ln redshift factor, 1 if the ray hit
+ * the disk plane inside the disk else 0, unused.
+ * Parameters: one FP32 vector of bhSurrogateParamCount() floats: for hidden
+ * layer l = 0..3 the 256 x 256 weight (row = output unit) then 256 biases,
+ * then the 16 x 256 head weight and 16 biases. */
+typedef struct BHSurrogate BHSurrogate;
+
+int bhSurrogateParamCount(void);
+
+/* New network on the current device, Xavier-uniform weights from `seed`,
+ * zero biases (blocking). */
+cudaError_t bhSurrogateCreate(BHSurrogate** s, unsigned seed);
+void bhSurrogateDestroy(BHSurrogate* s);
+
+/* Copy the FP32 parameter vector to / from host memory (blocking); setting
+ * parameters resets the optimiser state. */
+cudaError_t bhSurrogateGetParams(BHSurrogate* s, float* host);
+cudaError_t bhSurrogateSetParams(BHSurrogate* s, const float* host);
+
+/* The BF16 feature matrix (n x 256, row-major) of n input rows. */
+cudaError_t bhSurrogateFeatures(const float* in, void* features, int n, cudaStream_t stream);
+
+/* Head outputs (n x 16 floats) of n input rows.  fused != 0: the fused
+ * persistent tensor-core kernel used for rendering; fused == 0: the training
+ * path (one tensor-core GEMM per layer plus element-wise kernels). */
+cudaError_t bhSurrogateForward(BHSurrogate* s, const float* in, float* out, int n, int fused, cudaStream_t stream);
+
+/* Forward, loss and backward on n rays (n a multiple of 128; device inputs
+ * and targets); copies the gradient of the batch-mean loss (ParamCount
+ * floats) and the five batch-mean loss terms (class cross-entropy, escape
+ * direction, disk radius, disk redshift, confidence) to host memory
+ * (blocking).  Loss weights: 100 |escape error|^2 on escaped rays, 1 on the
+ * disk terms of disk-hit rays, 0.1 on the confidence cross-entropy whose
+ * target is 1 when the predicted class is right and, for escaped rays, the
+ * escape error is below 1e-3. */
+cudaError_t bhSurrogateGradients(BHSurrogate* s, const float* in, const float* tgt, int n, float* gradsHost,
+                                 float* lossHost);
+
+/* Trace `rays` rays with the FP32 RK4 tracer of this library over `views`
+ * random views of the parameter box (model uniform over the four families;
+ * a* U(-0.998, 0.998) and q U(0, 0.6) with a*^2 + q^2 <= 0.98 by rejection,
+ * zeroed where the family has no spin / charge; camera distance U(6, 60);
+ * inclination U(2, 88) deg; azimuth U(0, 360) deg; vertical FOV U(30, 90)
+ * deg, 16:9; disk on; balanced preset), directions uniform over each view's
+ * screen, all from `seed`; the ray set (inputs and targets) stays in device
+ * memory (blocking). */
+cudaError_t bhSurrogateGenerate(BHSurrogate* s, long long rays, int views, unsigned seed);
+
+/* Device pointers to the current ray set (rows of 8 floats) and its size. */
+cudaError_t bhSurrogateDataset(BHSurrogate* s, const float** in, const float** tgt, long long* n);
+
+/* Copy rows first .. first + count - 1 of the ray set to host memory (either
+ * pointer may be null; blocking). */
+cudaError_t bhSurrogateDatasetCopy(BHSurrogate* s, float* in, float* tgt, long long first, long long count);
+
+/* `steps` Adam steps (beta 0.9 / 0.999) on batches of `batch` rays (a
+ * multiple of 128) drawn from the ray set by a hash of (seed, step); the
+ * learning rate decays from lr to lr / 20 on a cosine.  lossHistory (may be
+ * null) receives 5 batch-mean loss terms per step (blocking). */
+cudaError_t bhSurrogateTrain(BHSurrogate* s, int steps, int batch, float lr, unsigned seed, float* lossHistory);
+
+/* Render one frame with the surrogate: same buffers and result layout as
+ * launchRenderPipeline.  Requires an orbit camera (looking at the hole, no
+ * roll: camRight.y == 0) and accumMode 0.  The fused kernel resolves the
+ * pixels it is sure of (escaped or captured without the disk, class
+ * probability and confidence >= 0.95, farther than 2 % from the critical
+ * curve); the rest, plus a held-out sample of 1 in 256 of the resolved
+ * pixels, go through the FP32 RK4 tracer; then bloom and tonemap.  The
+ * critical curve (per polar angle on the screen) is found by RK4 bisection
+ * once per metric, camera distance, inclination and field of view, and
+ * cached (that first call blocks). */
+cudaError_t bhSurrogateRender(BHSurrogate* s, uchar4* out, float4* accum, float4* bloomA, float4* bloomB,
+                              const RenderParams* p, cudaStream_t stream);
+
+/* Statistics of the last rendered frame (blocking). */
+typedef struct BHSurrogateStats
+{
+    unsigned pixels;          /* W * H */
+    unsigned rk4Pixels;       /* pixels traced by RK4 (fallback + held-out) */
+    unsigned heldOut;         /* held-out pixels compared */
+    unsigned heldOutOver1Lsb; /* held-out pixels whose RGBA8 differs by > 1 LSB */
+    unsigned heldOutOverTol;  /* held-out pixels with HDR error > 1e-3 relative */
+    float heldOutMaxAbs;      /* largest HDR difference on the held-out sample */
+} BHSurrogateStats;
+cudaError_t bhSurrogateFrameStats(BHSurrogate* s, BHSurrogateStats* stats);
+
 #ifdef __cplusplus
 }
 #endif

@@ -1,0 +1,249 @@
+"""The lensing surrogate through the C-ABI: features, the fused tensor-core
+inference kernel against the training path and the CPU oracle, gradients of
+the training loss against the CPU oracle, training on RK4-traced rays, and the
+surrogate frame (fused inference + RK4 for the rest)."""
+import ctypes as C
+
+import numpy as np
+import pytest
+
+import sg_oracle as SG
+from bhrt import lib, scenes
+from bhrt.device import Frame
+
+pytestmark = pytest.mark.gpu
+
+
+def _stream():
+    import torch
+    return C.c_void_p(torch.cuda.current_stream().cuda_stream)
+
+
+def _ptr(t):
+    return C.c_void_p(t.data_ptr())
+
+
+class Net:
+    def __init__(self, seed=1):
+        self.L = lib.load()
+        self.h = C.c_void_p()
+        assert self.L.bhSurrogateCreate(C.byref(self.h), seed) == 0
+        self.count = self.L.bhSurrogateParamCount()
+
+    def params(self):
+        p = np.zeros(self.count, dtype=np.float32)
+        assert self.L.bhSurrogateGetParams(self.h, p.ctypes.data_as(C.c_void_p)) == 0
+        return p
+
+    def set_params(self, p):
+        p = np.ascontiguousarray(p, dtype=np.float32)
+        assert self.L.bhSurrogateSetParams(self.h, p.ctypes.data_as(C.c_void_p)) == 0
+
+    def forward(self, inp, fused):
+        import torch
+        x = torch.as_tensor(inp, dtype=torch.float32, device="cuda").contiguous()
+        y = torch.zeros((x.shape[0], 16), dtype=torch.float32, device="cuda")
+        assert self.L.bhSurrogateForward(self.h, _ptr(x), _ptr(y), x.shape[0], int(fused), _stream()) == 0
+        torch.cuda.synchronize()
+        return y.cpu().numpy()
+
+    def close(self):
+        self.L.bhSurrogateDestroy(self.h)
+
+
+def _inputs(n, seed):
+    rng = np.random.default_rng(seed)
+    d = rng.normal(size=(n, 3))
+    d[:, 2] = np.abs(d[:, 2]) + 0.8
+    d /= np.linalg.norm(d, axis=1, keepdims=True)
+    x = np.zeros((n, 8), dtype=np.float32)
+    x[:, :3] = d
+    x[:, 3:7] = rng.uniform(-1, 1, size=(n, 4))
+    return x
+
+
+def _targets(inp, seed):
+    rng = np.random.default_rng(seed)
+    n = inp.shape[0]
+    t = np.zeros((n, 8), dtype=np.float32)
+    t[:, 0] = rng.integers(0, 3, size=n)
+    e = inp[:, :3] + rng.normal(scale=0.05, size=(n, 3))
+    t[:, 1:4] = e / np.linalg.norm(e, axis=1, keepdims=True)
+    hit = rng.random(n) < 0.5
+    t[:, 4] = np.where(hit, rng.uniform(0.3, 1.0, n), 0)
+    t[:, 5] = np.where(hit, rng.normal(scale=0.3, size=n), 0)
+    t[:, 6] = hit
+    return t
+
+
+def _features(inp):
+    import torch
+    x = torch.as_tensor(inp, device="cuda")
+    f = torch.zeros((x.shape[0], 256), dtype=torch.bfloat16, device="cuda")
+    assert lib.load().bhSurrogateFeatures(_ptr(x), _ptr(f), x.shape[0], _stream()) == 0
+    torch.cuda.synchronize()
+    return f.float().cpu().numpy()
+
+
+def test_features_match_oracle(cuda):
+    inp = _inputs(2048, 3)
+    got = _features(inp)
+    want = SG.bf16(SG.features(inp))
+    # one BF16 rounding step of values in [-1, 1], plus the angle-doubling error of the top bands
+    assert np.abs(got - want).max() <= 2.0 ** -8 + 1e-4
+    assert np.all(got[:, 231:] == 0)
+
+
+def test_fused_inference_matches_training_path_and_oracle(cuda):
+    net = Net(5)
+    try:
+        inp = _inputs(1000, 4)   # ragged: 7 full tiles + 104 rays
+        fused = net.forward(inp, True)
+        train = net.forward(inp, False)
+        scale = np.abs(train).max()
+        assert np.abs(fused - train).max() <= 1e-5 * scale + 1e-6
+        Y, _, _ = SG.forward(_features(inp), net.params())
+        rel = np.abs(fused - Y).max() / np.abs(Y).max()
+        print(f"fused vs training path {np.abs(fused - train).max():.3g}, vs oracle rel {rel:.3g}")
+        assert rel < 3e-2
+    finally:
+        net.close()
+
+
+def test_gradients_match_oracle(cuda):
+    import torch
+    net = Net(9)
+    try:
+        p = net.params()
+        rng = np.random.default_rng(2)
+        p[SG.HIDDEN * SG.HID:] += rng.normal(scale=0.05, size=p.size - SG.HIDDEN * SG.HID).astype(np.float32)
+        for l in range(SG.HIDDEN):   # non-zero biases exercise the bias path
+            p[l * SG.HID + 65536:(l + 1) * SG.HID] = rng.normal(scale=0.1, size=256)
+        net.set_params(p)
+        n = 256
+        inp = _inputs(n, 6)
+        tgt = _targets(inp, 7)
+        x = torch.as_tensor(inp, device="cuda")
+        t = torch.as_tensor(tgt, device="cuda")
+        g = np.zeros(net.count, dtype=np.float32)
+        loss = np.zeros(5, dtype=np.float32)
+        assert net.L.bhSurrogateGradients(net.h, _ptr(x), _ptr(t), n, g.ctypes.data_as(C.c_void_p),
+                                          loss.ctypes.data_as(C.c_void_p)) == 0
+        want, wloss = SG.gradients(_features(inp), p, inp.astype(np.float64), tgt.astype(np.float64))
+        print("loss gpu", loss, "oracle", wloss)
+        assert np.allclose(loss, wloss, rtol=2e-2, atol=1e-4)
+        blocks = []
+        for l in range(SG.HIDDEN + 1):
+            w0 = l * SG.HID
+            nw = 65536 if l < SG.HIDDEN else 16 * 256
+            nb = 256 if l < SG.HIDDEN else 16
+            blocks += [(f"W{l}", w0, w0 + nw), (f"b{l}", w0 + nw, w0 + nw + nb)]
+        for name, a, b in blocks:
+            err = np.linalg.norm(g[a:b] - want[a:b]) / max(np.linalg.norm(want[a:b]), 1e-12)
+            print(f"{name}: rel L2 {err:.3g}")
+            assert err < 5e-2, name
+    finally:
+        net.close()
+
+
+def _dataset(net, count):
+    n = C.c_longlong()
+    assert net.L.bhSurrogateDataset(net.h, None, None, C.byref(n)) == 0
+    count = min(count, n.value)
+    inp = np.zeros((count, 8), dtype=np.float32)
+    tgt = np.zeros((count, 8), dtype=np.float32)
+    assert net.L.bhSurrogateDatasetCopy(net.h, inp.ctypes.data_as(C.c_void_p), tgt.ctypes.data_as(C.c_void_p),
+                                        0, count) == 0
+    return inp, tgt
+
+
+def _metrics(y, inp, tgt):
+    cls = tgt[:, 0].astype(int)
+    pred = np.argmax(y[:, :3], axis=1)
+    esc = (cls == 0) & (pred == 0)
+    e = inp[:, :3] + y[:, 3:6]
+    e /= np.linalg.norm(e, axis=1, keepdims=True)
+    ang = np.linalg.norm(e - tgt[:, 1:4], axis=1)[esc]
+    return float((pred == cls).mean()), float(np.median(ang)) if ang.size else 0.0
+
+
+def test_train_on_rk4_rays(cuda):
+    net = Net(7)
+    held = Net(1)
+    try:
+        L = net.L
+        assert L.bhSurrogateGenerate(net.h, 64 * 8192, 64, 7) == 0
+        inp, tgt = _dataset(net, 4096)
+        frac = np.bincount(tgt[:, 0].astype(int), minlength=3) / len(tgt)
+        print("class fractions (escaped, captured, disk):", frac)
+        assert np.all(frac > 0.001)
+        assert np.allclose(np.linalg.norm(tgt[tgt[:, 0] == 0, 1:4], axis=1), 1, atol=1e-5)
+        steps = 300
+        hist = np.zeros((steps, 5), dtype=np.float32)
+        assert L.bhSurrogateTrain(net.h, steps, 8192, C.c_float(2e-3), 11, hist.ctypes.data_as(C.c_void_p)) == 0
+        first, last = hist[:5].sum(axis=1).mean(), hist[-20:].sum(axis=1).mean()
+        print(f"loss {first:.4f} -> {last:.4f}; final terms {hist[-20:].mean(axis=0)}")
+        assert np.all(np.isfinite(hist)) and last < 0.5 * first
+        # a fresh ray set of the same box: the trained network beats the untrained one
+        assert L.bhSurrogateGenerate(held.h, 16 * 4096, 16, 8) == 0
+        hin, htg = _dataset(held, 65536)
+        acc, ang = _metrics(net.forward(hin, True), hin, htg)
+        acc0, _ = _metrics(held.forward(hin, True), hin, htg)
+        print(f"held-out class accuracy {acc:.4f} (untrained {acc0:.4f}), median escape error {ang:.3g}")
+        assert acc > max(0.8, acc0 + 0.2)
+    finally:
+        net.close()
+        held.close()
+
+
+def _render(net, P):
+    import torch
+    f = Frame(P.width, P.height)
+    assert net.L.bhSurrogateRender(net.h, _ptr(f.out), _ptr(f.accum), _ptr(f.bloomA), _ptr(f.bloomB), C.byref(P),
+                                   _stream()) == 0
+    torch.cuda.synchronize()
+    st = np.zeros(6, dtype=np.uint32)
+    assert net.L.bhSurrogateFrameStats(net.h, st.ctypes.data_as(C.c_void_p)) == 0
+    return f.out.cpu().numpy(), f.accum.cpu().numpy(), st
+
+
+def _plain(P):
+    import torch
+    f = Frame(P.width, P.height)
+    f.pipeline(P)
+    torch.cuda.synchronize()
+    return f.out.cpu().numpy(), f.accum.cpu().numpy()
+
+
+def _kn_scene(derive, w, h, az=0.0):
+    return scenes.scene(derive, 3, 0.8, 0.3, w, h, 25.0, 15.0, 45.0, az_deg=az)
+
+
+def test_render_with_every_pixel_on_rk4_equals_plain_frame(cuda, derive):
+    net = Net(3)
+    try:
+        p = net.params()
+        p[SG.HIDDEN * SG.HID + 16 * 256 + 2] = 50.0   # head bias: every pixel predicted "touched the disk"
+        net.set_params(p)
+        P = _kn_scene(derive, 320, 180)
+        out, acc, st = _render(net, P)
+        pout, pacc = _plain(P)
+        assert st[0] == 320 * 180 and st[1] == 320 * 180
+        assert np.array_equal(acc, pacc)
+        assert np.array_equal(out, pout)
+    finally:
+        net.close()
+
+
+def test_render_statistics_are_consistent(cuda, derive):
+    net = Net(4)
+    try:
+        P = _kn_scene(derive, 480, 270, az=40.0)
+        out, acc, st = _render(net, P)
+        pout, _ = _plain(P)
+        n = 480 * 270
+        print("stats", st, "RGBA equal fraction", float((out == pout).all(axis=2).mean()))
+        assert st[0] == n and st[1] <= n and st[2] <= st[1] and st[3] <= st[2]
+        assert np.all(np.isfinite(acc))
+    finally:
+        net.close()
