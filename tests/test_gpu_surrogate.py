@@ -172,25 +172,29 @@ def test_train_on_rk4_rays(cuda):
     held = Net(1)
     try:
         L = net.L
-        assert L.bhSurrogateGenerate(net.h, 64 * 8192, 64, 7) == 0
+        assert L.bhSurrogateGenerate(net.h, 1024 * 512, 1024, 7) == 0
         inp, tgt = _dataset(net, 4096)
         frac = np.bincount(tgt[:, 0].astype(int), minlength=3) / len(tgt)
         print("class fractions (escaped, captured, disk):", frac)
         assert np.all(frac > 0.001)
         assert np.allclose(np.linalg.norm(tgt[tgt[:, 0] == 0, 1:4], axis=1), 1, atol=1e-5)
-        steps = 300
+        steps = 600
         hist = np.zeros((steps, 5), dtype=np.float32)
         assert L.bhSurrogateTrain(net.h, steps, 8192, C.c_float(2e-3), 11, hist.ctypes.data_as(C.c_void_p)) == 0
         first, last = hist[:5].sum(axis=1).mean(), hist[-20:].sum(axis=1).mean()
         print(f"loss {first:.4f} -> {last:.4f}; final terms {hist[-20:].mean(axis=0)}")
         assert np.all(np.isfinite(hist)) and last < 0.5 * first
-        # a fresh ray set of the same box: the trained network beats the untrained one
-        assert L.bhSurrogateGenerate(held.h, 16 * 4096, 16, 8) == 0
+        # a fresh ray set of the same box (other views): better than the majority class and
+        # than the untrained network, escape directions within a few hundredths of a radian
+        assert L.bhSurrogateGenerate(held.h, 64 * 1024, 64, 8) == 0
         hin, htg = _dataset(held, 65536)
         acc, ang = _metrics(net.forward(hin, True), hin, htg)
-        acc0, _ = _metrics(held.forward(hin, True), hin, htg)
-        print(f"held-out class accuracy {acc:.4f} (untrained {acc0:.4f}), median escape error {ang:.3g}")
-        assert acc > max(0.8, acc0 + 0.2)
+        acc0, ang0 = _metrics(held.forward(hin, True), hin, htg)
+        major = np.bincount(htg[:, 0].astype(int), minlength=3).max() / len(htg)
+        print(f"held-out class accuracy {acc:.4f} (majority {major:.4f}, untrained {acc0:.4f}), "
+              f"median escape error {ang:.3g} (untrained {ang0:.3g})")
+        assert acc > max(0.9, major + 0.05, acc0 + 0.05)
+        assert ang < 0.05 and ang < 0.5 * ang0
     finally:
         net.close()
         held.close()
