@@ -59,6 +59,7 @@ _SIGNATURES = {
     "bhSurrogateTrain": (_int, [_vp, _int, _int, C.c_float, C.c_uint, _vp]),
     "bhSurrogateRender": (_int, [_vp, _vp, _vp, _vp, _vp, _P, _vp]),
     "bhSurrogateFrameStats": (_int, [_vp, _vp]),
+    "bhSurrogateSetGate": (_int, [_vp, C.c_float, C.c_float, C.c_float, _int]),
     "bhVersion": (C.c_char_p, []),
 }
 

@@ -7,6 +7,7 @@
 // it renders use the reference's camera, sky and post-processing exactly as
 // launchRenderPipeline does.
 // ---------------------------------------------------------------------------
+#include <algorithm>
 #include <cmath>
 #include <cstdint>
 #include <cstring>
@@ -108,6 +109,9 @@ struct BHSurrogate
     float4* heldPred = nullptr;
     unsigned heldCap = 0;
     unsigned frames = 0;
+    // acceptance gate of the surrogate frame
+    float minProb = 0.95f, minConf = 0.95f, critBand = 0.02f;
+    int heldStride = kHeldStride;
     unsigned lastPixels = 0;
     // critical curve cache
     bool critValid = false;
@@ -194,12 +198,14 @@ cudaError_t criticalCurve(BHSurrogate* s, const RenderParams& P0, float* crit)
 
 cudaError_t ensureFrame(BHSurrogate* s, size_t pixels)
 {
-    if (pixels <= s->listCap) return cudaSuccess;
+    const size_t stride = s->heldStride > 0 ? (size_t)s->heldStride : pixels + 1;
+    const size_t want = std::min(pixels, pixels / stride * 2 + 4096);
+    if (pixels <= s->listCap && want <= s->heldCap) return cudaSuccess;
     if (s->list) cudaFree(s->list);
     if (s->heldPix) cudaFree(s->heldPix);
     if (s->heldPred) cudaFree(s->heldPred);
     s->list = nullptr; s->heldPix = nullptr; s->heldPred = nullptr; s->listCap = 0; s->heldCap = 0;
-    const unsigned cap = (unsigned)(pixels / kHeldStride * 2 + 4096);
+    const unsigned cap = (unsigned)want;
     cudaError_t e = cudaMalloc(&s->list, pixels * sizeof(unsigned));
     if (e == cudaSuccess) e = cudaMalloc(&s->heldPix, cap * sizeof(unsigned));
     if (e == cudaSuccess) e = cudaMalloc(&s->heldPred, cap * sizeof(float4));
@@ -454,16 +460,16 @@ cudaError_t bhSurrogateRender(BHSurrogate* s, uchar4* out, float4* accum, float4
     F.tp = bh_frame_params(P, BH_OUT_ACCUM, accum);
     sceneInputs(P, F.aN, F.qN, F.rN, F.iN);
     std::memcpy(F.crit, s->crit, sizeof(F.crit));
-    F.critBand = 0.02f;
-    F.minProb = 0.95f;
-    F.minConf = 0.95f;
+    F.critBand = s->critBand;
+    F.minProb = s->minProb;
+    F.minConf = s->minConf;
     F.list = s->list;
     F.listCount = s->counters;
     F.heldPix = s->heldPix;
     F.heldPred = s->heldPred;
     F.heldCount = s->counters + 1;
     F.heldCap = s->heldCap;
-    F.heldStride = kHeldStride;
+    F.heldStride = s->heldStride;
     F.frameSeed = ++s->frames;
     s->lastPixels = (unsigned)pixels;
     if ((e = cudaMemsetAsync(s->counters, 0, 64, stream)) != cudaSuccess) return e;
@@ -513,4 +519,16 @@ extern "C" cudaError_t bhSurrogateDatasetCopy(BHSurrogate* s, float* in, float* 
     if (e == cudaSuccess && tgt)
         e = cudaMemcpy(tgt, s->S.dsTgt + first * 8, (size_t)count * 8 * sizeof(float), cudaMemcpyDeviceToHost);
     return e;
+}
+
+extern "C" cudaError_t bhSurrogateSetGate(BHSurrogate* s, float minProb, float minConf, float critBand, int heldStride)
+{
+    if (!s || !(minProb >= 0.f && minProb <= 1.f) || !(minConf >= 0.f && minConf <= 1.f) ||
+        !(critBand >= 0.f && critBand < 1.f) || heldStride < 0)
+        return cudaErrorInvalidValue;
+    s->minProb = minProb;
+    s->minConf = minConf;
+    s->critBand = critBand;
+    s->heldStride = heldStride;
+    return cudaSuccess;
 }

@@ -3,13 +3,15 @@
 // the tensor cores: Fourier features -> 4 x (256 x 256 GEMM + GELU) -> head,
 // one launch, activations never leave shared memory.
 //
-// CTA = 10 warps, one per SM (shared memory ~198 KB, all 512 TMEM columns):
-//   warps 0-3  epilogue group 0: 128 rays (one per thread) of tile A0
-//   warps 4-7  epilogue group 1: 128 rays of tile A1
-//   warp 8     TMA producer: streams 128 x 64 weight chunks (16 KB) through a
-//              4-stage ring (the 4 hidden layers are one 1024 x 256 tensor)
-//   warp 9     MMA issuer: tcgen05.mma M=128 N=128 K=16, accumulators in TMEM
-//              (group g owns columns 256g .. 256g + 255)
+// CTA = 18 warps, one per SM (shared memory ~198 KB, all 512 TMEM columns):
+//   warps 0-7   epilogue group 0: tile A0 of 128 rays; warp w reads TMEM lane
+//               quarter w % 4 (rays 32 (w % 4) ..) and column half w / 4, so
+//               two warps share each ray and split its 256 columns
+//   warps 8-15  epilogue group 1: tile A1, the same way
+//   warp 16     TMA producer: streams 128 x 64 weight chunks (16 KB) through a
+//               5-stage ring (the 4 hidden layers are one 1024 x 256 tensor)
+//   warp 17     MMA issuer: tcgen05.mma M=128 N=128 K=16, accumulators in TMEM
+//               (group g owns columns 256g .. 256g + 255)
 // The two groups ping-pong: while group 0 turns layer l's accumulator into
 // layer l+1's BF16 operand (bias, GELU, 128-byte-swizzled stores), the tensor
 // core runs layer l of group 1, and the other way round.  Per tile pair the
@@ -33,11 +35,12 @@ using namespace bhsg;
 
 namespace {
 
-constexpr int kRing = 4;
+constexpr int kRing = 5;
 constexpr uint32_t kTileBytes = 128u * 256u * 2u;       // one group's operand: 128 rows x 256 BF16
 constexpr uint32_t kChunkBytes = 128u * 128u;           // 128 weight rows x 64 BF16
 constexpr uint32_t kHeadChunkBytes = 16u * 128u;        // 16 head rows x 64 BF16
-constexpr int kThreads = 320;
+constexpr int kThreads = 576;
+constexpr int kProducerWarp = 16, kMmaWarp = 17;
 constexpr uint32_t kSmemBytes = 2 * kTileBytes + kRing * kChunkBytes + 1024;
 
 struct Bars
@@ -167,7 +170,7 @@ sg_infer_kernel(const __grid_constant__ CUtensorMap tW, const __grid_constant__ 
 {
     extern __shared__ uint8_t smemRaw[];
     __shared__ Bars B;
-    __shared__ float sBias[kHidden * kWidth + kOut];
+    __shared__ __align__(16) float sBias[kHidden * kWidth + kOut];
     uint8_t* smem = reinterpret_cast<uint8_t*>((reinterpret_cast<uintptr_t>(smemRaw) + 1023) & ~uintptr_t(1023));
     uint8_t* tiles = smem;                       // 2 x 64 KB operands
     uint8_t* ring = smem + 2 * kTileBytes;       // 4 x 16 KB weight chunks
@@ -177,10 +180,10 @@ sg_infer_kernel(const __grid_constant__ CUtensorMap tW, const __grid_constant__ 
     if (threadIdx.x == 0)
     {
         for (int s = 0; s < kRing; ++s) { mbar_init(&B.full[s], 1); mbar_init(&B.empty[s], 1); }
-        for (int g = 0; g < 2; ++g) { mbar_init(&B.aReady[g], 128); mbar_init(&B.accFull[g], 1); }
+        for (int g = 0; g < 2; ++g) { mbar_init(&B.aReady[g], 256); mbar_init(&B.accFull[g], 1); }
         fence_barrier_init();
     }
-    if (warp == 8)
+    if (warp == kProducerWarp)
     {
         __syncwarp();
         tmem_alloc(&B.tmem, 512);
@@ -190,7 +193,7 @@ sg_infer_kernel(const __grid_constant__ CUtensorMap tW, const __grid_constant__ 
     tc_fence_after();
     const uint32_t tmem = B.tmem;
 
-    if (warp == 8)
+    if (warp == kProducerWarp)
     {
         if (lane == 0)
         {   // ---- TMA producer ----
@@ -226,7 +229,7 @@ sg_infer_kernel(const __grid_constant__ CUtensorMap tW, const __grid_constant__ 
                     if (!mbar_wait(&B.full[k % kRing], (k / kRing) & 1, err)) break;
         }
     }
-    else if (warp == 9)
+    else if (warp == kMmaWarp)
     {
         if (lane == 0)
         {   // ---- MMA issuer ----
@@ -262,7 +265,7 @@ sg_infer_kernel(const __grid_constant__ CUtensorMap tW, const __grid_constant__ 
     }
     else
     {   // ---- epilogue groups ----
-        const int g = warp >> 2, wq = warp & 3;
+        const int g = warp >> 3, wq = warp & 3, half = (warp >> 2) & 1;
         const uint32_t row = (uint32_t)(wq * 32 + lane);
         uint8_t* tile = tiles + g * kTileBytes;
         const uint32_t tl = tmem + (uint32_t)g * 256u + ((uint32_t)(wq * 32) << 16);
@@ -284,7 +287,8 @@ sg_infer_kernel(const __grid_constant__ CUtensorMap tW, const __grid_constant__ 
                 for (int k = 0; k < kIn; ++k) r.x[k] = valid ? __ldg(rawIn + (size_t)rid * 8 + k) : 0.f;
             }
 #pragma unroll 4
-            for (int j = 0; j < 32; ++j) st_chunk(tile, row, (uint32_t)j * 8u, sg_feature_chunk(r.x, j));
+            for (int j = half * 16; j < half * 16 + 16; ++j)
+                st_chunk(tile, row, (uint32_t)j * 8u, sg_feature_chunk(r.x, j));
             fence_async_smem();
             mbar_arrive(&B.aReady[g]);
 
@@ -296,7 +300,7 @@ sg_infer_kernel(const __grid_constant__ CUtensorMap tW, const __grid_constant__ 
                 tc_fence_after();
                 const float* bl = sBias + l * kWidth;
 #pragma unroll 1
-                for (int c = 0; c < kWidth; c += 32)
+                for (int c = half * 128; c < half * 128 + 128; c += 32)
                 {
                     float v[32];
                     tmem_ld32(tl + (uint32_t)c, v);
@@ -305,10 +309,12 @@ sg_infer_kernel(const __grid_constant__ CUtensorMap tW, const __grid_constant__ 
                     {
                         uint4 o;
                         const int b = c + q4 * 8;
-                        o.x = pack_gelu(v[q4 * 8 + 0] + bl[b + 0], v[q4 * 8 + 1] + bl[b + 1]);
-                        o.y = pack_gelu(v[q4 * 8 + 2] + bl[b + 2], v[q4 * 8 + 3] + bl[b + 3]);
-                        o.z = pack_gelu(v[q4 * 8 + 4] + bl[b + 4], v[q4 * 8 + 5] + bl[b + 5]);
-                        o.w = pack_gelu(v[q4 * 8 + 6] + bl[b + 6], v[q4 * 8 + 7] + bl[b + 7]);
+                        const float4 b0 = *reinterpret_cast<const float4*>(bl + b);
+                        const float4 b1 = *reinterpret_cast<const float4*>(bl + b + 4);
+                        o.x = pack_gelu(v[q4 * 8 + 0] + b0.x, v[q4 * 8 + 1] + b0.y);
+                        o.y = pack_gelu(v[q4 * 8 + 2] + b0.z, v[q4 * 8 + 3] + b0.w);
+                        o.z = pack_gelu(v[q4 * 8 + 4] + b1.x, v[q4 * 8 + 5] + b1.y);
+                        o.w = pack_gelu(v[q4 * 8 + 6] + b1.z, v[q4 * 8 + 7] + b1.w);
                         st_chunk(tile, row, (uint32_t)b, o);
                     }
                 }
@@ -321,25 +327,28 @@ sg_infer_kernel(const __grid_constant__ CUtensorMap tW, const __grid_constant__ 
             phF ^= 1u;
             if (!ok) break;
             tc_fence_after();
-            float y[kOut];
-            tmem_ld16(tl, y);
-            tc_fence_before();
+            if (half == 0)
+            {   // the head's 16 columns: read and used by the first column half only
+                float y[kOut];
+                tmem_ld16(tl, y);
+                tc_fence_before();
 #pragma unroll
-            for (int k = 0; k < kOut; ++k) y[k] += sBias[kHidden * kWidth + k];
-            if constexpr (FRAME)
-            {
-                frame_output(F, rid, valid, r, y);
-            }
-            else if (valid)
-            {
+                for (int k = 0; k < kOut; ++k) y[k] += sBias[kHidden * kWidth + k];
+                if constexpr (FRAME)
+                {
+                    frame_output(F, rid, valid, r, y);
+                }
+                else if (valid)
+                {
 #pragma unroll
-                for (int k = 0; k < kOut; ++k) rawOut[(size_t)rid * kOut + k] = y[k];
+                    for (int k = 0; k < kOut; ++k) rawOut[(size_t)rid * kOut + k] = y[k];
+                }
             }
         }
     }
     tc_fence_before();
     __syncthreads();
-    if (warp == 8)
+    if (warp == kProducerWarp)
     {
         __syncwarp();
         tmem_free(tmem, 512);

@@ -65,6 +65,16 @@ __device__ __forceinline__ uint64_t global_ns()
     return t;
 }
 
+// One suspending wait: the thread sleeps until the phase completes or about
+// `hintNs` nanoseconds pass (no issue slots spent spinning).
+__device__ __forceinline__ bool mbar_try_wait_sleep(uint64_t* bar, uint32_t parity, uint32_t hintNs)
+{
+    uint32_t ok;
+    asm volatile("{ .reg .pred p; mbarrier.try_wait.parity.shared::cta.b64 p, [%1], %2, %3; selp.u32 %0, 1, 0, p; }"
+                 : "=r"(ok) : "r"(smem_u32(bar)), "r"(parity), "r"(hintNs) : "memory");
+    return ok != 0;
+}
+
 // Wait for the phase with the given parity to complete, at most `limitNs`
 // nanoseconds.  On time-out sets bit 0 of *err and returns false.
 __device__ __forceinline__ bool mbar_wait(uint64_t* bar, uint32_t parity, unsigned* err,
@@ -72,17 +82,13 @@ __device__ __forceinline__ bool mbar_wait(uint64_t* bar, uint32_t parity, unsign
 {
     if (mbar_test(bar, parity)) return true;
     const uint64_t t0 = global_ns();
-    for (uint32_t i = 1;; ++i)
+    while (true)
     {
-        if (mbar_test(bar, parity)) return true;
-        if ((i & 255u) == 0)
+        if (mbar_try_wait_sleep(bar, parity, 200000u)) return true;
+        if (global_ns() - t0 > limitNs)
         {
-            if (global_ns() - t0 > limitNs)
-            {
-                atomicOr(err, 1u);
-                return false;
-            }
-            __nanosleep(64);
+            atomicOr(err, 1u);
+            return false;
         }
     }
 }

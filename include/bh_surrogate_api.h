@@ -126,6 +126,14 @@ cudaError_t bhSurrogateTrain(BHSurrogate* s, int steps, int batch, float lr, uns
 cudaError_t bhSurrogateRender(BHSurrogate* s, uchar4* out, float4* accum, float4* bloomA, float4* bloomB,
                               const RenderParams* p, cudaStream_t stream);
 
+/* Acceptance gate of bhSurrogateRender (defaults 0.95, 0.95, 0.02, 256): a
+ * pixel is resolved by the network only if its class probability is at least
+ * minProb, its confidence at least minConf and it lies farther than
+ * critBand (relative) from the critical curve; 1 in heldStride resolved
+ * pixels is also traced by RK4 and compared (0: none).  Lower thresholds trade
+ * accuracy for speed; heldStride 1 compares every resolved pixel. */
+cudaError_t bhSurrogateSetGate(BHSurrogate* s, float minProb, float minConf, float critBand, int heldStride);
+
 /* Statistics of the last rendered frame (blocking). */
 typedef struct BHSurrogateStats
 {
