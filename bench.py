@@ -24,6 +24,16 @@ whole job, plus frame ms.
   cpu_baseline  the reference's own tracer (src/trace.cuh built as host code,
              oracle/_ref) on the host cores, on a bounded pixel sample.
 
+  surrogate  (1 GPU only; --no-surrogate skips it) the learned lensing
+             surrogate: generate 16.7 M RK4-traced rays over 8192 views of the
+             batched-workload parameter box (seed 7), train 6000 Adam steps of
+             16384 rays, then 3840x2160 Kerr-Newman a*=0.8 q=0.3, r = 25,
+             inclination 75 deg, FOV 45 deg frames of the 300-frame orbit: plain
+             launchRenderPipeline vs bhSurrogateRender (median frame ms, pixels
+             within +-1 LSB of the plain frame, RK4 share) under the strict and a
+             permissive acceptance gate; fused tensor-core MLP throughput against
+             the measured BF16 peak.
+
 Multi-GPU: one process per GPU (torchrun); every rank renders its own 16-frame
 batch (frames offset in animation time), no collective on the data path
 ("scaling": "weak"); timing is the max over ranks.
@@ -56,6 +66,7 @@ def parse():
     ap.add_argument("--impl", default="b200", choices=["b200", "reference"])
     ap.add_argument("--no-cpu-baseline", action="store_true")
     ap.add_argument("--baseline-seconds", type=float, default=12.0)
+    ap.add_argument("--no-surrogate", action="store_true")
     return ap.parse_args()
 
 
@@ -261,6 +272,123 @@ def run_b200(args, rank, world, local_rank):
     return out, trace_total
 
 
+# ---------------------------------------------------------------------------
+# learned surrogate leg (single GPU): train, then 3840x2160 frames, plain vs surrogate
+# ---------------------------------------------------------------------------
+SG_W, SG_H = 3840, 2160
+SG_FRAMES = (0, 50, 100, 150, 200, 250)        # of the 300-frame orbit (azimuth 360 k / 300 deg)
+
+
+def surrogate_leg():
+    import ctypes as C
+    import torch
+    from bhrt import lib, scenes
+    from bhrt.device import Frame
+    L = lib.load()
+    sp = C.c_void_p(torch.cuda.current_stream().cuda_stream)
+    ptr = lambda t: C.c_void_p(t.data_ptr())  # noqa: E731
+    h = C.c_void_p()
+    lib.check(L.bhSurrogateCreate(C.byref(h), 7), "bhSurrogateCreate")
+    try:
+        views, rays, steps, batch = 8192, 8192 * 2048, 6000, 16384
+        t0 = time.perf_counter()
+        lib.check(L.bhSurrogateGenerate(h, rays, views, 7), "bhSurrogateGenerate")
+        t_gen = time.perf_counter() - t0
+        hist = np.zeros((steps, 5), dtype=np.float32)
+        t0 = time.perf_counter()
+        lib.check(L.bhSurrogateTrain(h, steps, batch, C.c_float(2e-3), 11, hist.ctypes.data_as(C.c_void_p)),
+                  "bhSurrogateTrain")
+        t_train = time.perf_counter() - t0
+        # fused tensor-core inference alone on one 4K frame of rays
+        n = SG_W * SG_H
+        x = torch.zeros((n, 8), device="cuda")
+        x[:, 2] = 1.0
+        y = torch.empty((n, 16), device="cuda")
+        e0, e1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+        for _ in range(2):
+            lib.check(L.bhSurrogateForward(h, ptr(x), ptr(y), n, 1, sp), "bhSurrogateForward")
+        torch.cuda.synchronize()
+        e0.record()
+        for _ in range(5):
+            L.bhSurrogateForward(h, ptr(x), ptr(y), n, 1, sp)
+        e1.record()
+        torch.cuda.synchronize()
+        mlp_ms = e0.elapsed_time(e1) / 5
+        del x, y
+        flops = 2.0 * (4 * 256 * 256 + 256 * 16) * n
+        peaks = {}
+        try:
+            peaks = json.load(open(os.path.join(ROOT, "MEASURED_PEAKS.json")))
+        except OSError:
+            pass
+        bf16_peak = peaks.get("bf16_tflops", 1590.0)
+        fa, fb = Frame(SG_W, SG_H), Frame(SG_W, SG_H)
+
+        def scene(k):
+            return scenes.scene(lib.derive, 3, 0.8, 0.3, SG_W, SG_H, 25.0, 15.0, 45.0, az_deg=360.0 * k / 300.0)
+
+        def timed(fn):
+            e0.record()
+            fn()
+            e1.record()
+            torch.cuda.synchronize()
+            return e0.elapsed_time(e1)
+
+        def sur(P):
+            lib.check(L.bhSurrogateRender(h, ptr(fb.out), ptr(fb.accum), ptr(fb.bloomA), ptr(fb.bloomB),
+                                          C.byref(P), sp), "bhSurrogateRender")
+
+        t0 = time.perf_counter()
+        sur(scene(0))                                   # first frame: critical curve by RK4 bisection
+        torch.cuda.synchronize()
+        t_first = time.perf_counter() - t0
+        gates = {"strict": (0.95, 0.95, 0.02, 256), "permissive": (0.5, 0.0, 0.02, 256)}
+        res = {}
+        plain_ms = []
+        for gname, g in gates.items():
+            lib.check(L.bhSurrogateSetGate(h, C.c_float(g[0]), C.c_float(g[1]), C.c_float(g[2]), g[3]), "gate")
+            sur_ms, within, rk4, held, held_bad = [], [], [], 0, 0
+            for k in SG_FRAMES:
+                P = scene(k)
+                fa.pipeline(P)
+                sur(P)
+                torch.cuda.synchronize()
+                if gname == "strict":
+                    plain_ms.append(timed(lambda: fa.pipeline(P)))
+                sur_ms.append(timed(lambda: sur(P)))
+                d = (fa.out[..., :3].int() - fb.out[..., :3].int()).abs().amax(dim=-1)
+                within.append(float((d <= 1).float().mean()))
+                st = np.zeros(6, dtype=np.uint32)
+                lib.check(L.bhSurrogateFrameStats(h, st.ctypes.data_as(C.c_void_p)), "stats")
+                rk4.append(float(st[1]) / (SG_W * SG_H))
+                held += int(st[2])
+                held_bad += int(st[3])
+            res[gname] = {"gate": {"min_prob": g[0], "min_conf": g[1], "crit_band": g[2], "held_stride": g[3]},
+                          "frame_ms": float(np.median(sur_ms)),
+                          "px_within_1lsb": float(np.min(within)),
+                          "rk4_pixel_frac": float(np.mean(rk4)),
+                          "held_out": held, "held_out_over_1lsb": held_bad}
+        pm = float(np.median(plain_ms))
+        for r in res.values():
+            r["speedup_vs_plain"] = pm / r["frame_ms"]
+            r["mrays_s"] = SG_W * SG_H / (r["frame_ms"] * 1e-3) / 1e6
+        mlp_tflops = flops / (mlp_ms * 1e-3) / 1e12
+        return {
+            "workload": "kn_a0.8_q0.3_r25_incl75_fov45_3840x2160_orbit (6 of 300 frames)",
+            "plain_frame_ms": pm, "plain_mrays_s": SG_W * SG_H / (pm * 1e-3) / 1e6,
+            "train": {"rays": rays, "views": views, "steps": steps, "batch": batch, "seed": 7,
+                      "generate_s": t_gen, "train_s": t_train, "final_loss": hist[-50:].mean(axis=0).tolist()},
+            "first_frame_s": t_first,
+            "gates": res,
+            "mlp": {"ms_per_4k_frame": mlp_ms,
+                    "roofline": {"bound": "tensor", "achieved": mlp_tflops, "peak": bf16_peak, "unit": "TFLOP/s",
+                                 "frac": mlp_tflops / bf16_peak,
+                                 "peak_source": "MEASURED_PEAKS.json bf16_tflops (burst)" if peaks else "fallback"}},
+        }
+    finally:
+        L.bhSurrogateDestroy(h)
+
+
 def main():
     args = parse()
     rank = int(os.environ.get("RANK", "0"))
@@ -293,6 +421,8 @@ def main():
                                "flops_per_frame": flops_step / len(frames),
                                "steps_per_ray": float(np.mean([c["steps_per_ray"] for c in census]))}
             out["cpu_baseline"] = base
+        if world == 1 and not args.no_surrogate:
+            out["surrogate"] = surrogate_leg()
         print(json.dumps(out))
     if world > 1:
         dist.barrier()
