@@ -98,6 +98,19 @@ class BHDerived(C.Structure):
                 ("clamped", C.c_int), ("naked", C.c_int)]
 
 
+class BHDeriveRequest(C.Structure):
+    _fields_ = [("model", C.c_int), ("M", C.c_float), ("aStar", C.c_float), ("q", C.c_float),
+                ("allowNaked", C.c_int)]
+
+
+DERIVE_REQ_DTYPE = np.dtype([("model", np.int32), ("M", np.float32), ("aStar", np.float32), ("q", np.float32),
+                             ("allowNaked", np.int32)])
+DERIVED_DTYPE = np.dtype([("a", np.float32), ("Q", np.float32), ("rPlus", np.float32), ("rMinus", np.float32),
+                          ("rPhoton", np.float32), ("rErgo", np.float32), ("rIsco", np.float32),
+                          ("clamped", np.int32), ("naked", np.int32)])
+assert DERIVE_REQ_DTYPE.itemsize == 20 and DERIVED_DTYPE.itemsize == 36
+
+
 PROBE_DTYPE = np.dtype([
     ("outcome", np.int32), ("cls", np.int32), ("steps", np.int32), ("diskSamples", np.int32),
     ("escDir", np.float32, (3,)), ("trans", np.float32), ("accum", np.float32, (3,)),

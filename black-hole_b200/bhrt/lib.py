@@ -24,6 +24,7 @@ _SIGNATURES = {
     "bhSanitizeRenderParams": (_int, [_P]),
     "bhValidateAndDerive": (None, [_int, C.POINTER(C.c_float), C.POINTER(C.c_float),
                                    C.POINTER(C.c_float), _int, C.POINTER(BHDerived)]),
+    "bhDeriveBatch": (_int, [_vp, _vp, _int, _vp]),
     "bhProbeGrid": (_int, [_vp, _P, _int, _int, _int, _vp]),
     "bhProbeRays": (_int, [_vp, _vp, _int, _P, _int, _vp]),
     "bhRenderHDR": (_int, [_vp, _P, _int, _vp]),

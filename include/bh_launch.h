@@ -101,6 +101,25 @@ int bhSanitizeRenderParams(RenderParams* p);
 void bhValidateAndDerive(int model, float* M, float* aStar, float* q, int allowNaked,
                          BHDerived* out);
 
+/* One black hole to derive on the device (the arguments of bhValidateAndDerive). */
+typedef struct BHDeriveRequest
+{
+    int model;
+    float M, aStar, q;
+    int allowNaked;
+} BHDeriveRequest;
+
+/* bhValidateAndDerive for n black holes on the GPU (device arrays): out[i]
+ * receives the derived quantities and requests[i].M / aStar / q are
+ * overwritten with the validated values, exactly as the host function
+ * updates its arguments.  Same results as the host function (and so as the
+ * reference's host code, metric.cuh:224-329) bit for bit, except rPhoton of
+ * Kerr / Kerr-Newman, whose acos and cos are rounded correctly here: one ulp
+ * of difference from the host libm's acos grows to a few ulps (within 1e-6
+ * relative); the numeric ISCO scan runs as one CTA per request.  No counterpart in the reference, which
+ * derives on the host per view. */
+cudaError_t bhDeriveBatch(BHDeriveRequest* requests, BHDerived* out, int n, cudaStream_t stream);
+
 /* ---- extensions ------------------------------------------------------- */
 
 /* Trace the nx*ny grid of pixel-centre rays of the camera in `p` and write
