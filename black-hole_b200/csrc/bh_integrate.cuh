@@ -424,13 +424,16 @@ BH_DEV KerrEval<R> kerr_rhs(const CamFrame<R>& F, const KerrConsts<R>& k, R r, R
 {
     const R M = F.M, a2 = F.a2;
     s = max_p(s, R(1e-4f));                 // pole guard
-    R r2 = r * r;
-    R Sig = r2 + a2 * c * c;
+    R r2, a2c;
+    mul2_p(r, a2, r, c, r2, a2c);
+    R Sig = r2 + a2c * c;
     R DelRaw = r * (r - R(2) * M) + F.a2Q2;
     R Del = max_p(DelRaw, R(1e-6f));
     R Pp = k.E * r2 + k.c1;                 // E (r^2 + a^2) - a Lz
     R is = rcp_p(s);
-    R is2 = is * is;
+    R iS = rcp_p(Sig);
+    R is2, iS2;
+    mul2_p(is, iS, is, iS, is2, iS2);
     R B = k.Lz * is - k.aE * s;
     R iDel = rcp_p(Del);
     R PiD = Pp * iDel;
@@ -440,15 +443,13 @@ BH_DEV KerrEval<R> kerr_rhs(const CamFrame<R>& F, const KerrConsts<R>& k, R r, R
     R dDel = R(2) * (r - M);
     R Wr = -PiD * (R(2) * k.twoE * r - PiD * dDel);   // dP = 2 r E
     R Wth = R(-2) * B * c * (k.Lz * is2 + k.aE);
-    R iS = rcp_p(Sig);
-    R iS2 = iS * iS;
     R mh = R(-0.5f) * iS;
     R KiS2 = o.K * iS2;
-    o.d.r = Del * pr * iS;
-    o.d.th = pth * iS;
+    mul2_p(Del * pr, pth, iS, iS, o.d.r, o.d.th);
     o.d.ph = ((k.Lz * is2 - k.aE) + F.a * PiD) * iS;
-    o.d.pr = mh * (dDel * pr * pr + Wr) + r * KiS2;
-    o.d.pth = mh * Wth - a2 * s * c * KiS2;
+    R u0, u1;
+    mul2_p(r, -(a2 * s * c), KiS2, KiS2, u0, u1);
+    fma2_p(mh, dDel * pr * pr + Wr, Wth, u0, u1, o.d.pr, o.d.pth);
     o.Pp = Pp;
     o.iDelT = (DelRaw >= R(1e-5f)) ? iDel : R(1e5f);
     o.iS = iS;
@@ -622,28 +623,35 @@ struct KerrRay
             }
         }
 
-        // classic RK4
+        // classic RK4; the (r, theta) and (p_r, p_theta) halves of every stage
+        // update are independent pairs with a shared coefficient (packed FMAs)
         const R hh = R(0.5f) * h;
-        R sx, cx;
-        R yr = r + hh * d1.r, yth = th + hh * d1.th, ypr = pr + hh * d1.pr, ypth = pth + hh * d1.pth;
+        R sx, cx, yr, yth, ypr, ypth;
+        fma2_p(hh, d1.r, d1.th, r, th, yr, yth);
+        fma2_p(hh, d1.pr, d1.pth, pr, pth, ypr, ypth);
         sincos_stage(yth, sx, cx);
         KerrDeriv<R> d2 = kerr_rhs(F, k, yr, sx, cx, ypr, ypth).d;
-        R sr = d1.r + R(2) * d2.r, sth = d1.th + R(2) * d2.th, sph = d1.ph + R(2) * d2.ph;
-        R spr = d1.pr + R(2) * d2.pr, spth = d1.pth + R(2) * d2.pth;
-        yr = r + hh * d2.r; yth = th + hh * d2.th; ypr = pr + hh * d2.pr; ypth = pth + hh * d2.pth;
+        R sr, sth, spr, spth, sph = d1.ph + R(2) * d2.ph;
+        fma2_p(R(2), d2.r, d2.th, d1.r, d1.th, sr, sth);
+        fma2_p(R(2), d2.pr, d2.pth, d1.pr, d1.pth, spr, spth);
+        fma2_p(hh, d2.r, d2.th, r, th, yr, yth);
+        fma2_p(hh, d2.pr, d2.pth, pr, pth, ypr, ypth);
         sincos_stage(yth, sx, cx);
         KerrDeriv<R> d3 = kerr_rhs(F, k, yr, sx, cx, ypr, ypth).d;
-        sr += R(2) * d3.r; sth += R(2) * d3.th; sph += R(2) * d3.ph;
-        spr += R(2) * d3.pr; spth += R(2) * d3.pth;
-        yr = r + h * d3.r; yth = th + h * d3.th; ypr = pr + h * d3.pr; ypth = pth + h * d3.pth;
+        fma2_p(R(2), d3.r, d3.th, sr, sth, sr, sth);
+        fma2_p(R(2), d3.pr, d3.pth, spr, spth, spr, spth);
+        sph += R(2) * d3.ph;
+        fma2_p(h, d3.r, d3.th, r, th, yr, yth);
+        fma2_p(h, d3.pr, d3.pth, pr, pth, ypr, ypth);
         sincos_stage(yth, sx, cx);
         KerrDeriv<R> d4 = kerr_rhs(F, k, yr, sx, cx, ypr, ypth).d;
         const R h6 = h * R(1.0 / 6.0);
-        r += h6 * (sr + d4.r);
-        th += h6 * (sth + d4.th);
+        R t0, t1, t2, t3;
+        add2_p(sr, sth, d4.r, d4.th, t0, t1);
+        add2_p(spr, spth, d4.pr, d4.pth, t2, t3);
+        fma2_p(h6, t0, t1, r, th, r, th);
+        fma2_p(h6, t2, t3, pr, pth, pr, pth);
         ph += h6 * (sph + d4.ph);
-        pr += h6 * (spr + d4.pr);
-        pth += h6 * (spth + d4.pth);
         return finish_step(P, F, h, rS, thS, drS, dthS, d4.r, d4.th, d4.ph);
     }
 
@@ -678,7 +686,9 @@ struct KerrRay
         {
             R sp, cp;
             sincos_fast(ph, sp, cp);
-            f3 pos = v3((float)(r * s * cp), (float)(r * c), (float)(-r * s * sp));
+            R rs = r * s, px, pz;
+            mul2_p(rs, -rs, cp, sp, px, pz);
+            f3 pos = v3((float)px, (float)(r * c), (float)pz);
             if (trans > 0.01f)
                 disk_segment<STATS>(P, (float)k.E, (float)k.Lz, prevPos, pos, (float)(F.diskTime - tFlight),
                                     accum, trans, tally);

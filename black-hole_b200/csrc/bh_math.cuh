@@ -130,6 +130,42 @@ BH_DEV float  min_p(float a, float b)   { return fminf(a, b); }
 BH_DEV double min_p(double a, double b) { return fmin(a, b); }
 BH_DEV float  max_p(float a, float b)   { return fmaxf(a, b); }
 BH_DEV double max_p(double a, double b) { return fmax(a, b); }
+// Two independent a * x_i + y_i sharing a: one packed FP32x2 FMA on sm_100
+// (each component rounded exactly as a scalar FMA), two FMAs in FP64.
+BH_DEV void fma2_p(float a, float x0, float x1, float y0, float y1, float& o0, float& o1)
+{
+    const float2 v = __ffma2_rn(make_float2(a, a), make_float2(x0, x1), make_float2(y0, y1));
+    o0 = v.x;
+    o1 = v.y;
+}
+BH_DEV void fma2_p(double a, double x0, double x1, double y0, double y1, double& o0, double& o1)
+{
+    o0 = fma(a, x0, y0);
+    o1 = fma(a, x1, y1);
+}
+// Two independent sums / products (packed in FP32).
+BH_DEV void add2_p(float x0, float x1, float y0, float y1, float& o0, float& o1)
+{
+    const float2 v = __fadd2_rn(make_float2(x0, x1), make_float2(y0, y1));
+    o0 = v.x;
+    o1 = v.y;
+}
+BH_DEV void add2_p(double x0, double x1, double y0, double y1, double& o0, double& o1)
+{
+    o0 = x0 + y0;
+    o1 = x1 + y1;
+}
+BH_DEV void mul2_p(float x0, float x1, float y0, float y1, float& o0, float& o1)
+{
+    const float2 v = __fmul2_rn(make_float2(x0, x1), make_float2(y0, y1));
+    o0 = v.x;
+    o1 = v.y;
+}
+BH_DEV void mul2_p(double x0, double x1, double y0, double y1, double& o0, double& o1)
+{
+    o0 = x0 * y0;
+    o1 = x1 * y1;
+}
 BH_DEV bool   finite_p(float x)  { return isfinite(x); }
 BH_DEV bool   finite_p(double x) { return isfinite(x); }
 
