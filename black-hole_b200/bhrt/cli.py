@@ -6,6 +6,8 @@
     python black-hole_b200/bhrt/cli.py sweep --scene kn4k --frames 120 --step 12 --width 960 \\
         --height 540 --outdir frames/
     python black-hole_b200/bhrt/cli.py render --scene kn1080 --repeat 5      (timing)
+    python black-hole_b200/bhrt/cli.py batch --scene pair1080 --frames 16 --repeat 3   (one queue)
+    python black-hole_b200/bhrt/cli.py mlp --rays 2097152 --repeat 3      (surrogate MLP timing)
 
 Replaces the reference application's interactive loop (src/main.cpp): the
 orbit camera, body orientation and quality presets become arguments; frames
@@ -30,6 +32,8 @@ def named(name, frame, width, height):
     if name in ("kerr1080", "kn1080"):
         fr = scenes.kerr_pair_1080(d, width or 1920, height or 1080)
         return fr[(0 if name == "kerr1080" else 8) + (frame % 8)]
+    if name == "pair1080":
+        return scenes.kerr_pair_1080(d, width or 1920, height or 1080)[frame % 16]
     if name == "kn4k":
         return scenes.kn_sweep_4k(d, width or 3840, height or 2160, frame_ids=[frame % 120])[0]
     if name == "batch":
@@ -63,10 +67,59 @@ def render(P, precision, repeat, out_path):
     return times
 
 
+def render_batch(views, repeat):
+    """All views in one bhRenderBatch call (one work queue), timed."""
+    import ctypes as C
+    import torch
+    from bhrt.abi import BHView
+    from bhrt.device import Frame
+    fs = [Frame(P.width, P.height) for P in views]
+    arr = (BHView * len(views))()
+    for i, (P, f) in enumerate(zip(views, fs)):
+        arr[i].params = P
+        arr[i].out, arr[i].accum = f.out.data_ptr(), f.accum.data_ptr()
+        arr[i].bloomA, arr[i].bloomB = f.bloomA.data_ptr(), f.bloomB.data_ptr()
+    sp = C.c_void_p(torch.cuda.current_stream().cuda_stream)
+    times = []
+    for _ in range(max(1, repeat)):
+        e0, e1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+        e0.record()
+        lib.check(lib.load().bhRenderBatch(arr, len(views), sp), "bhRenderBatch")
+        e1.record()
+        torch.cuda.synchronize()
+        times.append(e0.elapsed_time(e1))
+    return times
+
+
+def time_mlp(rays, repeat):
+    """The fused tensor-core surrogate inference on `rays` synthetic input rows (untrained network)."""
+    import ctypes as C
+    import torch
+    L = lib.load()
+    h = C.c_void_p()
+    lib.check(L.bhSurrogateCreate(C.byref(h), 7), "bhSurrogateCreate")
+    x = torch.zeros((rays, 8), device="cuda")
+    x[:, 2] = 1.0
+    y = torch.empty((rays, 16), device="cuda")
+    sp = C.c_void_p(torch.cuda.current_stream().cuda_stream)
+    times = []
+    for _ in range(max(1, repeat)):
+        e0, e1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+        e0.record()
+        lib.check(L.bhSurrogateForward(h, C.c_void_p(x.data_ptr()), C.c_void_p(y.data_ptr()), rays, 1, sp),
+                  "bhSurrogateForward")
+        e1.record()
+        torch.cuda.synchronize()
+        times.append(e0.elapsed_time(e1))
+    L.bhSurrogateDestroy(h)
+    return times
+
+
 def main(argv=None):
     ap = argparse.ArgumentParser(description=__doc__, formatter_class=argparse.RawDescriptionHelpFormatter)
-    ap.add_argument("cmd", choices=["render", "sweep", "info"])
-    ap.add_argument("--scene", default=None, help="schw320 | kerr1080 | kn1080 | kn4k | batch")
+    ap.add_argument("cmd", choices=["render", "sweep", "batch", "mlp", "info"])
+    ap.add_argument("--rays", type=int, default=3840 * 2160)
+    ap.add_argument("--scene", default=None, help="schw320 | kerr1080 | kn1080 | pair1080 | kn4k | batch")
     ap.add_argument("--frame", type=int, default=0)
     ap.add_argument("--frames", type=int, default=120)
     ap.add_argument("--step", type=int, default=1)
@@ -106,6 +159,20 @@ def main(argv=None):
         t = render(P, prec, a.repeat, a.out)
         print(f"{P.width}x{P.height} {MODEL_NAMES[P.model]} {a.precision}: {min(t):.3f} ms (best of {len(t)})"
               + (f" -> {a.out}" if a.out else ""))
+        return 0
+    if a.cmd == "mlp":
+        t = time_mlp(a.rays, a.repeat)
+        flop = 2.0 * (4 * 256 * 256 + 256 * 16) * a.rays
+        print(f"fused surrogate MLP, {a.rays} rays: {min(t):.3f} ms (best of {len(t)}), "
+              f"{flop / min(t) / 1e9:.1f} TFLOP/s")
+        return 0
+    if a.cmd == "batch":
+        views = [named(a.scene, k, a.width, a.height) if a.scene else custom(a)
+                 for k in range(a.frame, a.frames, max(1, a.step))]
+        t = render_batch(views, a.repeat)
+        npx = sum(P.width * P.height for P in views)
+        print(f"{len(views)} views, {npx / 1e6:.2f} Mpx in one batch: {min(t):.3f} ms (best of {len(t)}), "
+              f"{npx / min(t) / 1e3:.1f} Mrays/s")
         return 0
     # sweep
     if a.outdir:
