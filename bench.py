@@ -26,6 +26,11 @@ whole job, plus frame ms.
   cpu_baseline  the reference's own tracer (src/trace.cuh built as host code,
              oracle/_ref) on the host cores, on a bounded pixel sample.
 
+  mixed_precision_4k, batch_256_views  (1 GPU only; --no-configs skips them)
+             frame ms of plain FP32 vs the mixed-precision mode on the
+             3840x2160 near-extremal Kerr-Newman elevation sweep, and the 256
+             random views of seed 1234 as one batch / CUDA graph vs 256
+             pipeline calls.
   surrogate  (1 GPU only; --no-surrogate skips it) the learned lensing
              surrogate: generate 16.7 M RK4-traced rays over 8192 views of the
              batched-workload parameter box (seed 7), train 6000 Adam steps of
@@ -69,6 +74,7 @@ def parse():
     ap.add_argument("--no-cpu-baseline", action="store_true")
     ap.add_argument("--baseline-seconds", type=float, default=12.0)
     ap.add_argument("--no-surrogate", action="store_true")
+    ap.add_argument("--no-configs", action="store_true")
     return ap.parse_args()
 
 
@@ -418,6 +424,87 @@ def surrogate_leg():
         L.bhSurrogateDestroy(h)
 
 
+# ---------------------------------------------------------------------------
+# configuration legs (single GPU): mixed precision at 4K, the 256-view batch
+# ---------------------------------------------------------------------------
+def mixed_leg():
+    """3840x2160 Kerr-Newman a*=0.998 (0.995 after the clamp) q=0.05, r=12, FOV 50, elevation sweep:
+    frame ms of plain FP32 and of the mixed-precision mode on 5 of the 120 sweep frames."""
+    import torch
+    from bhrt import lib, scenes
+    from bhrt.abi import BH_PREC_FP32, BH_PREC_MIXED
+    from bhrt.device import Frame
+    ids = (0, 30, 60, 90, 119)
+    frames = scenes.kn_sweep_4k(lib.derive, 3840, 2160, frames=120, frame_ids=ids)
+    f = Frame(3840, 2160)
+    e0, e1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+    res = {}
+    for name, prec in (("fp32", BH_PREC_FP32), ("mixed", BH_PREC_MIXED)):
+        ms = []
+        for P in frames:
+            f.pipeline(P, prec)
+            e0.record()
+            f.pipeline(P, prec)
+            e1.record()
+            torch.cuda.synchronize()
+            ms.append(e0.elapsed_time(e1))
+        res[name] = {"frame_ms": float(np.median(ms)), "mrays_s": 3840 * 2160 / (np.median(ms) * 1e-3) / 1e6,
+                     "frame_ms_by_elevation_deg": {str(round(89.0 * k / 119, 1)): m for k, m in zip(ids, ms)}}
+    res["workload"] = "kn_a0.998_q0.05_r12_fov50_3840x2160_sweep (frames 0, 30, 60, 90, 119 of 120)"
+    res["mixed_over_fp32_time"] = res["mixed"]["frame_ms"] / res["fp32"]["frame_ms"]
+    return res
+
+
+def batch256_leg():
+    """The 256 random views of seed 1234 (all four families, 128x72 .. 1920x1080): one bhRenderBatch
+    call vs 256 launchRenderPipeline calls, and the CUDA-graph replay."""
+    import ctypes as C
+    import torch
+    from bhrt import lib, scenes
+    from bhrt.abi import BHView
+    from bhrt.device import Frame
+    L = lib.load()
+    views = scenes.batch_views(lib.derive, 256, 1234)
+    fs = [Frame(P.width, P.height) for P in views]
+    arr = (BHView * len(views))()
+    for i, (P, f) in enumerate(zip(views, fs)):
+        arr[i].params = P
+        arr[i].out, arr[i].accum = f.out.data_ptr(), f.accum.data_ptr()
+        arr[i].bloomA, arr[i].bloomB = f.bloomA.data_ptr(), f.bloomB.data_ptr()
+    sp = C.c_void_p(torch.cuda.current_stream().cuda_stream)
+    npx = sum(P.width * P.height for P in views)
+    e0, e1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+
+    def timed(fn, reps=3):
+        fn()
+        torch.cuda.synchronize()
+        ts = []
+        for _ in range(reps):
+            e0.record()
+            fn()
+            e1.record()
+            torch.cuda.synchronize()
+            ts.append(e0.elapsed_time(e1))
+        return float(np.median(ts))
+
+    def seq():
+        for P, f in zip(views, fs):
+            f.pipeline(P)
+
+    g = C.c_void_p()
+    lib.check(L.bhBatchGraphCreate(C.byref(g), arr, len(views)), "bhBatchGraphCreate")
+    try:
+        t_seq = timed(seq)
+        t_batch = timed(lambda: lib.check(L.bhRenderBatch(arr, len(views), sp), "bhRenderBatch"))
+        t_graph = timed(lambda: lib.check(L.bhBatchGraphLaunch(g, sp), "bhBatchGraphLaunch"))
+    finally:
+        L.bhBatchGraphDestroy(g)
+    mr = lambda t: npx / (t * 1e-3) / 1e6  # noqa: E731
+    return {"workload": "batch_views seed 1234: 256 views, %.1f Mpx" % (npx / 1e6),
+            "sequential_ms": t_seq, "batch_ms": t_batch, "graph_ms": t_graph,
+            "sequential_mrays_s": mr(t_seq), "batch_mrays_s": mr(t_batch), "graph_mrays_s": mr(t_graph)}
+
+
 def main():
     args = parse()
     rank = int(os.environ.get("RANK", "0"))
@@ -450,6 +537,9 @@ def main():
                                "flops_per_frame": flops_step / len(frames),
                                "steps_per_ray": float(np.mean([c["steps_per_ray"] for c in census]))}
             out["cpu_baseline"] = base
+        if world == 1 and not args.no_configs:
+            out["mixed_precision_4k"] = mixed_leg()
+            out["batch_256_views"] = batch256_leg()
         if world == 1 and not args.no_surrogate:
             out["surrogate"] = surrogate_leg()
         print(json.dumps(out))
