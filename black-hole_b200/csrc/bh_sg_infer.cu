@@ -3,24 +3,29 @@
 // the tensor cores: Fourier features -> 4 x (256 x 256 GEMM + GELU) -> head,
 // one launch, activations never leave shared memory.
 //
-// CTA = 18 warps, one per SM (shared memory ~198 KB, all 512 TMEM columns):
-//   warps 0-7   epilogue group 0: tile A0 of 128 rays; warp w reads TMEM lane
-//               quarter w % 4 (rays 32 (w % 4) ..) and column half w / 4, so
-//               two warps share each ray and split its 256 columns
-//   warps 8-15  epilogue group 1: tile A1, the same way
-//   warp 16     TMA producer: streams 128 x 64 weight chunks (16 KB) through a
-//               5-stage ring (the 4 hidden layers are one 1024 x 256 tensor)
-//   warp 17     MMA issuer: tcgen05.mma M=128 N=128 K=16, accumulators in TMEM
-//               (group g owns columns 256g .. 256g + 255)
+// CTA pairs (clusters of 2, tcgen05 cta_group::2): a pair computes 256-row
+// tiles, 128 rows in each CTA, with M = 256 MMAs issued by the leader (cluster
+// rank 0); each CTA streams only its half of every weight chunk (128 of the
+// 256 output rows), so the per-SM weight stream is half that of a single-SM
+// 128-row tile.  Each CTA = 18 warps, one CTA per SM (~202 KB shared memory,
+// all 512 TMEM columns, allocated for the pair):
+//   warps 0-7   epilogue group 0: this CTA's 128 rows of tile pair A0; warp w
+//               reads TMEM lane quarter w % 4 and column half w / 4
+//   warps 8-15  epilogue group 1: the same for A1
+//   warp 16     TMA producer: this CTA's 128 x 64 weight chunk (16 KB) into a
+//               5-stage ring, completing on the leader's barrier
+//   warp 17     MMA issuer (leader only): tcgen05.mma M=256 N=256 K=16,
+//               accumulators in both CTAs' TMEM (group g owns columns 256g ..)
 // The two groups ping-pong: while group 0 turns layer l's accumulator into
 // layer l+1's BF16 operand (bias, GELU, 128-byte-swizzled stores), the tensor
-// core runs layer l of group 1, and the other way round.  Per tile pair the
-// producer and the issuer walk the same chunk sequence:
-//   for l in 0..3: for g in 0..1: for kb in 0..3: for half in 0..1: W_l[half rows, kb cols]
-//   then for g in 0..1: for kb in 0..3: W_head[:, kb cols]
-// Barriers: full/empty per ring stage, aReady[g] (128 epilogue arrivals: the
-// operand of the next layer is in shared memory and the accumulator is free),
-// accFull[g] (MMA commit: layer done).  All waits are bounded (bh_tc.cuh).
+// core runs group 1's layer l, and the other way round.  Producers and the
+// issuer walk the same chunk sequence per tile pair:
+//   for l in 0..3: for g in 0..1: for kb in 0..3: W_l[rank half of rows, kb cols]
+//   then for g in 0..1: for kb in 0..3: W_head (32 rows, 16 per CTA, the upper 16 zero)
+// Barriers: full[s] (leader: both CTAs' chunk bytes), empty[s] and accFull[g]
+// (multicast MMA commits to both CTAs), aReady[g] (leader: 512 epilogue
+// arrivals from both CTAs -- the operand of the next layer is in shared memory
+// and the accumulator is free).  All waits are bounded (bh_tc.cuh).
 // ---------------------------------------------------------------------------
 #include <cuda.h>
 #include <cuda_bf16.h>
@@ -172,94 +177,88 @@ sg_infer_kernel(const __grid_constant__ CUtensorMap tW, const __grid_constant__ 
     __shared__ Bars B;
     __shared__ __align__(16) float sBias[kHidden * kWidth + kOut];
     uint8_t* smem = reinterpret_cast<uint8_t*>((reinterpret_cast<uintptr_t>(smemRaw) + 1023) & ~uintptr_t(1023));
-    uint8_t* tiles = smem;                       // 2 x 64 KB operands
-    uint8_t* ring = smem + 2 * kTileBytes;       // 4 x 16 KB weight chunks
+    uint8_t* tiles = smem;                       // 2 x 64 KB operands (this CTA's 128 rows of each group)
+    uint8_t* ring = smem + 2 * kTileBytes;       // weight chunks: this CTA's half of the N rows
     const int warp = threadIdx.x >> 5, lane = threadIdx.x & 31;
+    const uint32_t rank = cluster_rank();        // 0: leader (issues the MMAs), 1: peer
+    const unsigned pair = blockIdx.x >> 1, pairs = gridDim.x >> 1;
 
     for (int i = threadIdx.x; i < kHidden * kWidth + kOut; i += kThreads) sBias[i] = bias[i];
     if (threadIdx.x == 0)
     {
         for (int s = 0; s < kRing; ++s) { mbar_init(&B.full[s], 1); mbar_init(&B.empty[s], 1); }
-        for (int g = 0; g < 2; ++g) { mbar_init(&B.aReady[g], 256); mbar_init(&B.accFull[g], 1); }
+        for (int g = 0; g < 2; ++g) { mbar_init(&B.aReady[g], 512); mbar_init(&B.accFull[g], 1); }
         fence_barrier_init();
     }
     if (warp == kProducerWarp)
     {
         __syncwarp();
-        tmem_alloc(&B.tmem, 512);
+        tmem_alloc_pair(&B.tmem, 512);
     }
     tc_fence_before();
-    __syncthreads();
+    cluster_sync();
     tc_fence_after();
     const uint32_t tmem = B.tmem;
 
     if (warp == kProducerWarp)
     {
         if (lane == 0)
-        {   // ---- TMA producer ----
+        {   // ---- TMA producer (both CTAs): this CTA's half of every weight chunk ----
             tma_prefetch_desc(&tW);
             tma_prefetch_desc(&tH);
             uint32_t q = 0;
             bool ok = true;
             for (unsigned it = 0; it < iters && ok; ++it)
-            {
                 for (int l = 0; l <= kHidden && ok; ++l)
                     for (int g = 0; g < 2 && ok; ++g)
-                        for (int kb = 0; kb < 4 && ok; ++kb)
-                            for (int h = 0; h < (l < kHidden ? 2 : 1) && ok; ++h, ++q)
-                            {
-                                const uint32_t s = q % kRing;
-                                if (q >= kRing && !(ok = mbar_wait(&B.empty[s], ((q / kRing) - 1) & 1, err))) break;
-                                uint8_t* dst = ring + s * kChunkBytes;
-                                if (l < kHidden)
-                                {
-                                    mbar_expect_tx(&B.full[s], kChunkBytes);
-                                    tma_load_2d(dst, &tW, &B.full[s], kb * 64, l * 256 + h * 128);
-                                }
-                                else
-                                {
-                                    mbar_expect_tx(&B.full[s], kHeadChunkBytes);
-                                    tma_load_2d(dst, &tH, &B.full[s], kb * 64, 0);
-                                }
-                            }
-            }
-            // drain: the last loads must land before the CTA may exit
-            if (ok && q > 0)
+                        for (int kb = 0; kb < 4 && ok; ++kb, ++q)
+                        {
+                            const uint32_t s = q % kRing;
+                            if (q >= kRing && !(ok = mbar_wait_cluster(&B.empty[s], ((q / kRing) - 1) & 1, err)))
+                                break;
+                            uint8_t* dst = ring + s * kChunkBytes;
+                            const uint32_t leaderFull = mapa_shared(&B.full[s], 0);
+                            const uint32_t bytes = l < kHidden ? kChunkBytes : kHeadChunkBytes;
+                            if (rank == 0) mbar_expect_tx(&B.full[s], 2u * bytes);
+                            if (l < kHidden) tma_load_2d_pair(dst, &tW, leaderFull, kb * 64, l * 256 + (int)rank * 128);
+                            else tma_load_2d_pair(dst, &tH, leaderFull, kb * 64, (int)rank * kOut);
+                        }
+            // drain: the last loads must land before the pair may exit
+            if (rank == 0 && ok && q > 0)
                 for (uint32_t k = (q > kRing ? q - kRing : 0); k < q; ++k)
-                    if (!mbar_wait(&B.full[k % kRing], (k / kRing) & 1, err)) break;
+                    if (!mbar_wait_cluster(&B.full[k % kRing], (k / kRing) & 1, err)) break;
         }
     }
     else if (warp == kMmaWarp)
     {
-        if (lane == 0)
-        {   // ---- MMA issuer ----
-            const uint32_t idH = idesc_bf16_f32(128), idHead = idesc_bf16_f32(kOut);
+        if (lane == 0 && rank == 0)
+        {   // ---- MMA issuer (leader): M = 256 over the pair ----
+            const uint32_t idH = idesc_bf16_f32_m256(256), idHead = idesc_bf16_f32_m256(2 * kOut);
             uint32_t q = 0, phA[2] = {0, 0};
             bool ok = true;
             for (unsigned it = 0; it < iters && ok; ++it)
                 for (int l = 0; l <= kHidden && ok; ++l)
                     for (int g = 0; g < 2 && ok; ++g)
                     {
-                        if (!(ok = mbar_wait(&B.aReady[g], phA[g], err))) break;
+                        if (!(ok = mbar_wait_cluster(&B.aReady[g], phA[g], err))) break;
                         phA[g] ^= 1u;
                         tc_fence_after();
                         const uint32_t aBase = smem_u32(tiles + g * kTileBytes);
                         const uint32_t d = tmem + (uint32_t)g * 256u;
-                        for (int kb = 0; kb < 4 && ok; ++kb)
-                            for (int h = 0; h < (l < kHidden ? 2 : 1) && ok; ++h, ++q)
-                            {
-                                const uint32_t s = q % kRing;
-                                if (!(ok = mbar_wait(&B.full[s], (q / kRing) & 1, err))) break;
-                                tc_fence_after();
-                                const uint32_t bBase = smem_u32(ring + s * kChunkBytes);
-                                const uint32_t aBlk = aBase + (uint32_t)kb * 16384u;
+                        for (int kb = 0; kb < 4 && ok; ++kb, ++q)
+                        {
+                            const uint32_t s = q % kRing;
+                            if (!(ok = mbar_wait_cluster(&B.full[s], (q / kRing) & 1, err))) break;
+                            tc_fence_after();
+                            const uint32_t bBase = smem_u32(ring + s * kChunkBytes);
+                            const uint32_t aBlk = aBase + (uint32_t)kb * 16384u;
 #pragma unroll
-                                for (int j = 0; j < 4; ++j)
-                                    mma_bf16(d + (uint32_t)h * 128u, sdesc_sw128(aBlk + j * 32), sdesc_sw128(bBase + j * 32),
-                                             l < kHidden ? idH : idHead, kb > 0 || j > 0);
-                                mma_commit(&B.empty[s]);
-                            }
-                        mma_commit(&B.accFull[g]);
+                            for (int j = 0; j < 4; ++j)
+                                mma_bf16_pair(d, sdesc_sw128(aBlk + j * 32), sdesc_sw128(bBase + j * 32),
+                                              l < kHidden ? idH : idHead, kb > 0 || j > 0);
+                            mma_commit_pair(&B.empty[s]);
+                        }
+                        mma_commit_pair(&B.accFull[g]);
                     }
         }
     }
@@ -269,12 +268,13 @@ sg_infer_kernel(const __grid_constant__ CUtensorMap tW, const __grid_constant__ 
         const uint32_t row = (uint32_t)(wq * 32 + lane);
         uint8_t* tile = tiles + g * kTileBytes;
         const uint32_t tl = tmem + (uint32_t)g * 256u + ((uint32_t)(wq * 32) << 16);
+        const uint32_t aReadyLeader = mapa_shared(&B.aReady[g], 0);
         uint32_t phF = 0;
         bool ok = true;
         for (unsigned it = 0; it < iters && ok; ++it)
         {
-            const unsigned tileIdx = (it * gridDim.x + blockIdx.x) * 2u + (unsigned)g;
-            const unsigned rid = tileIdx * 128u + row;
+            const unsigned superTile = (it * pairs + pair) * 2u + (unsigned)g;
+            const unsigned rid = superTile * 256u + rank * 128u + row;
             const bool valid = rid < n;
             RayIn r;
             if constexpr (FRAME)
@@ -290,11 +290,11 @@ sg_infer_kernel(const __grid_constant__ CUtensorMap tW, const __grid_constant__ 
             for (int j = half * 16; j < half * 16 + 16; ++j)
                 st_chunk(tile, row, (uint32_t)j * 8u, sg_feature_chunk(r.x, j));
             fence_async_smem();
-            mbar_arrive(&B.aReady[g]);
+            mbar_arrive_cluster(aReadyLeader);
 
             for (int l = 0; l < kHidden && ok; ++l)
             {
-                ok = __all_sync(0xffffffffu, mbar_wait(&B.accFull[g], phF, err));
+                ok = __all_sync(0xffffffffu, mbar_wait_cluster(&B.accFull[g], phF, err));
                 phF ^= 1u;
                 if (!ok) break;
                 tc_fence_after();
@@ -320,10 +320,10 @@ sg_infer_kernel(const __grid_constant__ CUtensorMap tW, const __grid_constant__ 
                 }
                 tc_fence_before();
                 fence_async_smem();
-                mbar_arrive(&B.aReady[g]);
+                mbar_arrive_cluster(aReadyLeader);
             }
             if (!ok) break;
-            ok = __all_sync(0xffffffffu, mbar_wait(&B.accFull[g], phF, err));
+            ok = __all_sync(0xffffffffu, mbar_wait_cluster(&B.accFull[g], phF, err));
             phF ^= 1u;
             if (!ok) break;
             tc_fence_after();
@@ -347,11 +347,11 @@ sg_infer_kernel(const __grid_constant__ CUtensorMap tW, const __grid_constant__ 
         }
     }
     tc_fence_before();
-    __syncthreads();
+    cluster_sync();
     if (warp == kProducerWarp)
     {
         __syncwarp();
-        tmem_free(tmem, 512);
+        tmem_free_pair(tmem, 512);
     }
 }
 
@@ -362,29 +362,43 @@ cudaError_t sg_infer_launch(const SgInferArgs& a, const SgFrame* frame, cudaStre
     if (a.n == 0) return cudaSuccess;
     CUtensorMap tW, tH;
     cudaError_t e = bh_tensor_map_bf16(&tW, a.Whidden, kHidden * kWidth, kWidth, kWidth, 128);
-    if (e == cudaSuccess) e = bh_tensor_map_bf16(&tH, a.Whead, kOut, kWidth, kWidth, kOut);
+    // the head as 32 rows (16 per CTA of a pair; rows 16..31 are zero in the weight buffer)
+    if (e == cudaSuccess) e = bh_tensor_map_bf16(&tH, a.Whead, 2 * kOut, kWidth, kWidth, kOut);
     if (e != cudaSuccess) return e;
     int dev = 0, sms = 0;
     if ((e = cudaGetDevice(&dev)) != cudaSuccess) return e;
     if ((e = cudaDeviceGetAttribute(&sms, cudaDevAttrMultiProcessorCount, dev)) != cudaSuccess) return e;
-    const unsigned tiles = (a.n + 127u) / 128u;
-    const unsigned pairs = (tiles + 1u) / 2u;
-    const unsigned grid = std::min<unsigned>((unsigned)sms, pairs);
-    const unsigned iters = (pairs + grid - 1u) / grid;
+    const unsigned superTiles = (a.n + 255u) / 256u;            // 256 rays per pair and group
+    const unsigned want = (superTiles + 1u) / 2u;               // pair-iterations of work
+    const unsigned pairs = std::max(1u, std::min<unsigned>((unsigned)sms / 2u, want));
+    const unsigned iters = (want + pairs - 1u) / pairs;
     SgFrame F{};
     if (frame) F = *frame;
+    cudaLaunchConfig_t cfg{};
+    cudaLaunchAttribute attr[1];
+    attr[0].id = cudaLaunchAttributeClusterDimension;
+    attr[0].val.clusterDim.x = 2;
+    attr[0].val.clusterDim.y = 1;
+    attr[0].val.clusterDim.z = 1;
+    cfg.gridDim = dim3(2u * pairs);
+    cfg.blockDim = dim3(kThreads);
+    cfg.dynamicSmemBytes = kSmemBytes;
+    cfg.stream = s;
+    cfg.attrs = attr;
+    cfg.numAttrs = 1;
     if (frame)
     {
         auto k = sg_infer_kernel<true>;
         if ((e = cudaFuncSetAttribute(k, cudaFuncAttributeMaxDynamicSharedMemorySize, kSmemBytes))) return e;
-        k<<<grid, kThreads, kSmemBytes, s>>>(tW, tH, F, a.bias, nullptr, nullptr, a.n, iters, a.err);
+        e = cudaLaunchKernelEx(&cfg, k, tW, tH, F, a.bias, (const float*)nullptr, (float*)nullptr, a.n, iters, a.err);
     }
     else
     {
         auto k = sg_infer_kernel<false>;
         if ((e = cudaFuncSetAttribute(k, cudaFuncAttributeMaxDynamicSharedMemorySize, kSmemBytes))) return e;
-        k<<<grid, kThreads, kSmemBytes, s>>>(tW, tH, F, a.bias, a.rawIn, a.rawOut, a.n, iters, a.err);
+        e = cudaLaunchKernelEx(&cfg, k, tW, tH, F, a.bias, a.rawIn, a.rawOut, a.n, iters, a.err);
     }
+    if (e != cudaSuccess) return e;
     return cudaGetLastError();
 }
 

@@ -201,6 +201,105 @@ __device__ __forceinline__ void tmem_ld16(uint32_t taddr, float* v)
     for (int i = 0; i < 16; ++i) v[i] = __uint_as_float(r[i]);
 }
 
+// ---- CTA pairs (cluster of 2, tcgen05 cta_group::2) ---------------------------
+// A pair computes M = 256 tiles: each CTA holds 128 rows of A and half of the
+// N rows of B at the same shared-memory offsets; the leader (cluster rank 0)
+// issues the MMAs, and each CTA's TMEM receives its own 128 rows.
+__device__ __forceinline__ uint32_t cluster_rank()
+{
+    uint32_t r;
+    asm volatile("mov.u32 %0, %%cluster_ctarank;" : "=r"(r));
+    return r;
+}
+
+// shared::cluster address of the same variable in CTA `rank` of the cluster
+__device__ __forceinline__ uint32_t mapa_shared(const void* p, uint32_t rank)
+{
+    uint32_t out;
+    asm volatile("mapa.shared::cluster.u32 %0, %1, %2;" : "=r"(out) : "r"(smem_u32(p)), "r"(rank));
+    return out;
+}
+
+__device__ __forceinline__ void cluster_sync()
+{
+    asm volatile("barrier.cluster.arrive.release.aligned;\n\tbarrier.cluster.wait.acquire.aligned;" ::: "memory");
+}
+
+// arrive (release, cluster scope) on a barrier given by its shared::cluster address
+__device__ __forceinline__ void mbar_arrive_cluster(uint32_t clusterAddr)
+{
+    asm volatile("mbarrier.arrive.release.cluster.shared::cluster.b64 _, [%0];" ::"r"(clusterAddr) : "memory");
+}
+
+// bounded wait with cluster-scope acquire (arrivals that come from the peer CTA)
+__device__ __forceinline__ bool mbar_wait_cluster(uint64_t* bar, uint32_t parity, unsigned* err,
+                                                  uint64_t limitNs = 2000000000ull)
+{
+    const uint64_t t0 = global_ns();
+    while (true)
+    {
+        uint32_t ok;
+        asm volatile("{ .reg .pred p; mbarrier.try_wait.parity.acquire.cluster.shared::cta.b64 p, [%1], %2, %3; "
+                     "selp.u32 %0, 1, 0, p; }"
+                     : "=r"(ok) : "r"(smem_u32(bar)), "r"(parity), "r"(200000u) : "memory");
+        if (ok) return true;
+        if (global_ns() - t0 > limitNs)
+        {
+            atomicOr(err, 1u);
+            return false;
+        }
+    }
+}
+
+// 2-D tiled load into this CTA's shared memory, completing on a barrier of
+// either CTA of the pair (its shared::cluster address); no multicast.
+__device__ __forceinline__ void tma_load_2d_pair(void* dst, const void* tmap, uint32_t barCluster, int x, int y)
+{
+    asm volatile(
+        "cp.async.bulk.tensor.2d.cta_group::2.shared::cluster.global.mbarrier::complete_tx::bytes "
+        "[%0], [%1, {%3, %4}], [%2];"
+        ::"r"(smem_u32(dst)), "l"(reinterpret_cast<uint64_t>(tmap)), "r"(barCluster), "r"(x), "r"(y)
+        : "memory");
+}
+
+__device__ __forceinline__ void tmem_alloc_pair(uint32_t* slot, uint32_t cols)
+{
+    asm volatile("tcgen05.alloc.cta_group::2.sync.aligned.shared::cta.b32 [%0], %1;"
+                 ::"r"(smem_u32(slot)), "r"(cols) : "memory");
+    asm volatile("tcgen05.relinquish_alloc_permit.cta_group::2.sync.aligned;" ::: "memory");
+}
+
+__device__ __forceinline__ void tmem_free_pair(uint32_t base, uint32_t cols)
+{
+    asm volatile("tcgen05.dealloc.cta_group::2.sync.aligned.b32 %0, %1;" ::"r"(base), "r"(cols) : "memory");
+}
+
+// Instruction descriptor for the pair: BF16 x BF16 -> FP32, K-major, M = 256.
+__host__ __device__ constexpr uint32_t idesc_bf16_f32_m256(uint32_t n)
+{
+    return (1u << 4) | (1u << 7) | (1u << 10) | ((n >> 3) << 17) | ((256u >> 4) << 24);
+}
+
+__device__ __forceinline__ void mma_bf16_pair(uint32_t dTmem, uint64_t aDesc, uint64_t bDesc, uint32_t idesc,
+                                              bool accumulate)
+{
+    asm volatile(
+        "{ .reg .pred p; setp.ne.b32 p, %4, 0;\n\t"
+        "tcgen05.mma.cta_group::2.kind::f16 [%0], %1, %2, %3, p; }"
+        ::"r"(dTmem), "l"(aDesc), "l"(bDesc), "r"(idesc), "r"((uint32_t)accumulate)
+        : "memory");
+}
+
+// Arrive on the barrier at this offset in both CTAs of the pair once the MMAs
+// issued so far have completed.
+__device__ __forceinline__ void mma_commit_pair(uint64_t* bar)
+{
+    asm volatile(
+        "{ .reg .b16 m; mov.b16 m, 3;\n\t"
+        "tcgen05.commit.cta_group::2.mbarrier::arrive::one.shared::cluster.multicast::cluster.b64 [%0], m; }"
+        ::"r"(smem_u32(bar)) : "memory");
+}
+
 // Byte offset of element (row, col) in a 128-row-group operand stored as
 // 64-column blocks of `rows` x 128 B with the 128-byte swizzle.
 __host__ __device__ __forceinline__ uint32_t sw128_offset(uint32_t row, uint32_t col, uint32_t rows)
