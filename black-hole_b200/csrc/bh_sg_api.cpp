@@ -240,7 +240,8 @@ cudaError_t bhSurrogateCreate(BHSurrogate** out, unsigned seed)
     if (e == cudaSuccess) e = cudaMalloc(&S.loss, 8 * sizeof(float));
     if (e == cudaSuccess) e = cudaMalloc(&s->counters, 64);
     if (e == cudaSuccess) e = bh_tc_error_word(&S.err);
-    if (e == cudaSuccess) e = cudaMemset(S.W, 0, kWCount * 2);
+    // every set-up write goes on the network's stream, ordered with the kernels that follow
+    if (e == cudaSuccess) e = cudaMemsetAsync(S.W, 0, kWCount * 2, s->stream);
     if (e != cudaSuccess) { freeAll(s); return e; }
     // Xavier-uniform weights, zero biases
     std::vector<float> p(SgLayout::count(), 0.f);
@@ -279,9 +280,9 @@ cudaError_t bhSurrogateSetParams(BHSurrogate* s, const float* host)
     SgState& S = s->S;
     const size_t pc = (size_t)SgLayout::count() * sizeof(float);
     cudaError_t e = cudaStreamSynchronize(s->stream);
-    if (e == cudaSuccess) e = cudaMemcpy(S.params, host, pc, cudaMemcpyHostToDevice);
-    if (e == cudaSuccess) e = cudaMemset(S.adamM, 0, pc);
-    if (e == cudaSuccess) e = cudaMemset(S.adamV, 0, pc);
+    if (e == cudaSuccess) e = cudaMemcpyAsync(S.params, host, pc, cudaMemcpyHostToDevice, s->stream);
+    if (e == cudaSuccess) e = cudaMemsetAsync(S.adamM, 0, pc, s->stream);
+    if (e == cudaSuccess) e = cudaMemsetAsync(S.adamV, 0, pc, s->stream);
     if (e == cudaSuccess) e = sg_pack_weights(S, s->stream);
     if (e == cudaSuccess) e = cudaStreamSynchronize(s->stream);
     S.step = 0;
@@ -314,7 +315,9 @@ cudaError_t bhSurrogateGradients(BHSurrogate* s, const float* in, const float* t
 {
     if (!s || !in || !tgt || n <= 0 || n % 128) return cudaErrorInvalidValue;
     SgState& S = s->S;
-    cudaError_t e = sg_gradients(S, in, tgt, n, s->stream);
+    // the caller's inputs may come from any stream: wait for all prior work
+    cudaError_t e = cudaDeviceSynchronize();
+    if (e == cudaSuccess) e = sg_gradients(S, in, tgt, n, s->stream);
     if (e == cudaSuccess) e = cudaStreamSynchronize(s->stream);
     if (e == cudaSuccess) e = checkErrWord(s);
     if (e == cudaSuccess && gradsHost)

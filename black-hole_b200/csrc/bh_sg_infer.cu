@@ -60,9 +60,12 @@ __device__ __forceinline__ void st_chunk(uint8_t* tile, uint32_t row, uint32_t c
     *reinterpret_cast<uint4*>(tile + sw128_offset(row, col, 128)) = v;
 }
 
-__device__ __forceinline__ uint32_t pack_gelu(float a, float b)
+// (acc + bias) / 2 in one packed FP32 FMA (bias2 = bias / 2; exact halving),
+// BF16 rounding, GELU from the halved input (bit-identical to gelu2)
+__device__ __forceinline__ uint32_t pack_gelu(float a, float b, float ba2, float bb2)
 {
-    __nv_bfloat162 h = gelu2(__floats2bfloat162_rn(a, b));
+    const float2 z = __ffma2_rn(make_float2(a, b), make_float2(0.5f, 0.5f), make_float2(ba2, bb2));
+    __nv_bfloat162 h = gelu2_half(__floats2bfloat162_rn(z.x, z.y));
     return *reinterpret_cast<uint32_t*>(&h);
 }
 
@@ -183,7 +186,9 @@ sg_infer_kernel(const __grid_constant__ CUtensorMap tW, const __grid_constant__ 
     const uint32_t rank = cluster_rank();        // 0: leader (issues the MMAs), 1: peer
     const unsigned pair = blockIdx.x >> 1, pairs = gridDim.x >> 1;
 
-    for (int i = threadIdx.x; i < kHidden * kWidth + kOut; i += kThreads) sBias[i] = bias[i];
+    // hidden-layer biases are kept halved (the epilogue forms (acc + bias) / 2); head biases as they are
+    for (int i = threadIdx.x; i < kHidden * kWidth + kOut; i += kThreads)
+        sBias[i] = i < kHidden * kWidth ? 0.5f * bias[i] : bias[i];
     if (threadIdx.x == 0)
     {
         for (int s = 0; s < kRing; ++s) { mbar_init(&B.full[s], 1); mbar_init(&B.empty[s], 1); }
@@ -311,10 +316,10 @@ sg_infer_kernel(const __grid_constant__ CUtensorMap tW, const __grid_constant__ 
                         const int b = c + q4 * 8;
                         const float4 b0 = *reinterpret_cast<const float4*>(bl + b);
                         const float4 b1 = *reinterpret_cast<const float4*>(bl + b + 4);
-                        o.x = pack_gelu(v[q4 * 8 + 0] + b0.x, v[q4 * 8 + 1] + b0.y);
-                        o.y = pack_gelu(v[q4 * 8 + 2] + b0.z, v[q4 * 8 + 3] + b0.w);
-                        o.z = pack_gelu(v[q4 * 8 + 4] + b1.x, v[q4 * 8 + 5] + b1.y);
-                        o.w = pack_gelu(v[q4 * 8 + 6] + b1.z, v[q4 * 8 + 7] + b1.w);
+                        o.x = pack_gelu(v[q4 * 8 + 0], v[q4 * 8 + 1], b0.x, b0.y);
+                        o.y = pack_gelu(v[q4 * 8 + 2], v[q4 * 8 + 3], b0.z, b0.w);
+                        o.z = pack_gelu(v[q4 * 8 + 4], v[q4 * 8 + 5], b1.x, b1.y);
+                        o.w = pack_gelu(v[q4 * 8 + 6], v[q4 * 8 + 7], b1.z, b1.w);
                         st_chunk(tile, row, (uint32_t)b, o);
                     }
                 }

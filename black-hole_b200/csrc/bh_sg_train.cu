@@ -48,7 +48,7 @@ __global__ void act_kernel(const float2* __restrict__ Z, __nv_bfloat162* __restr
     const long long i = blockIdx.x * (long long)blockDim.x + threadIdx.x;
     if (i >= pairs) return;
     const float2 z = Z[i];
-    X[i] = gelu2(__floats2bfloat162_rn(z.x, z.y));
+    X[i] = gelu2_half(__floats2bfloat162_rn(0.5f * z.x, 0.5f * z.y));   // = gelu2 of bf16(z), exactly
 }
 
 // dZ = dX * gelu'(bf16(Z)) for 64 rows per block, thread = column; column sums -> db
@@ -288,7 +288,7 @@ cudaError_t sg_pack_weights(SgState& S, cudaStream_t s)
     return cudaGetLastError();
 }
 
-cudaError_t sg_reserve(SgState& S, int n)
+cudaError_t sg_reserve(SgState& S, int n, cudaStream_t s)
 {
     if (n <= S.cap) return cudaSuccess;
     sg_free_batch(S);
@@ -305,7 +305,7 @@ cudaError_t sg_reserve(SgState& S, int n)
     take((void**)&S.T0, nw * 2);
     take((void**)&S.T1, nw * 2);
     take((void**)&S.headTmp, (size_t)128 * kWidth * 4);
-    if (e == cudaSuccess) e = cudaMemset(S.dYt, 0, (size_t)128 * n * 2);
+    if (e == cudaSuccess) e = cudaMemsetAsync(S.dYt, 0, (size_t)128 * n * 2, s);   // ordered with its users
     if (e != cudaSuccess) { sg_free_batch(S); return e; }
     S.cap = n;
     return cudaSuccess;
@@ -335,7 +335,7 @@ static cudaError_t transpose(const void* in, void* out, int rows, int cols, cuda
 // forward pass through the GEMM path (training form): Y = net(in)
 cudaError_t sg_forward_train(SgState& S, const float* in, int n, cudaStream_t s)
 {
-    cudaError_t e = sg_reserve(S, n);
+    cudaError_t e = sg_reserve(S, n, s);
     if (e == cudaSuccess) e = sg_features(in, S.X[0], n, s);
     const size_t ww = (size_t)kWidth * kWidth;
     for (int l = 0; l < kHidden && e == cudaSuccess; ++l)

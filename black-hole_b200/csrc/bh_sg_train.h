@@ -54,7 +54,8 @@ struct SgState
 
 cudaError_t sg_features(const float* in, void* X0, int n, cudaStream_t s);
 cudaError_t sg_pack_weights(SgState& S, cudaStream_t s);
-cudaError_t sg_reserve(SgState& S, int n);
+// grows the per-batch scratch to n rays; the zero fill is enqueued on s
+cudaError_t sg_reserve(SgState& S, int n, cudaStream_t s);
 void sg_free_batch(SgState& S);
 cudaError_t sg_forward_train(SgState& S, const float* in, int n, cudaStream_t s);
 cudaError_t sg_gradients(SgState& S, const float* in, const float* tgt, int n, cudaStream_t s);

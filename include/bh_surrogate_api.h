@@ -83,7 +83,8 @@ cudaError_t bhSurrogateForward(BHSurrogate* s, const float* in, float* out, int 
  * and targets); copies the gradient of the batch-mean loss (ParamCount
  * floats) and the five batch-mean loss terms (class cross-entropy, escape
  * direction, disk radius, disk redshift, confidence) to host memory
- * (blocking).  Loss weights: 100 |escape error|^2 on escaped rays, 1 on the
+ * (blocking; the call first waits for all work on the device, so the inputs
+ * may come from any stream).  Loss weights: 100 |escape error|^2 on escaped rays, 1 on the
  * disk terms of disk-hit rays, 0.1 on the confidence cross-entropy whose
  * target is 1 when the predicted class is right and, for escaped rays, the
  * escape error is below 1e-3. */
