@@ -14,9 +14,10 @@ whole job, plus frame ms.
              tiles, then each frame's bloom + tonemap), timed with CUDA events
              on the launch stream; max over ranks.  The per-frame form
              (bhRenderAccum + bhPostProcess per frame) is reported beside it.
-  e2e        the reference-facing call: launchRenderPipeline with RenderParams
-             from the host and the RGBA8 frame copied back to pinned host memory
-             inside the timed region.
+  e2e        the reference-facing call: launchRenderPipeline per frame with
+             RenderParams from the host, each RGBA8 frame copied back to pinned
+             host memory (on a copy stream, overlapping the next frame) inside
+             the timed region.
   roofline   the tracing kernel (dominant): algorithmic FLOPs / its event time
              against the measured FP32 FMA peak.  Algorithmic FLOPs follow the
              reference's work on the same inputs: RK4 steps x 420 (Kerr family)
@@ -193,7 +194,6 @@ def run_b200(args, rank, world, local_rank):
     frames = workload(lib.derive, rank)
     nF = len(frames)
     fs = [Frame(W, H, device=dev) for _ in frames]
-    f = fs[0]
     L = lib.load()
     stream = torch.cuda.current_stream()
     sp = C.c_void_p(stream.cuda_stream)
@@ -256,17 +256,25 @@ def run_b200(args, rank, world, local_rank):
     # tracing time inside the batch: the step minus its 16 bloom + tonemap passes
     batch_trace_total = total_ms - float(np.median(post_ms)) * nF * args.steps
 
-    # e2e: the reference-facing call, params from the host, RGBA8 back to pinned host memory
-    host = torch.empty((H, W, 4), dtype=torch.uint8, pin_memory=True)
+    # e2e: the reference-facing call per frame, params from the host, each RGBA8 frame read back to
+    # pinned host memory on a copy stream (overlapping the next frame's tracing); the step ends when
+    # the last read-back has landed
+    hosts = [torch.empty((H, W, 4), dtype=torch.uint8, pin_memory=True) for _ in range(nF)]
+    cstream = torch.cuda.Stream(device=dev)
     e2 = [(torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)) for _ in range(args.steps)]
     for s in range(-1, args.steps):
         flush.zero_()
         if s >= 0:
             e2[s][0].record(stream)
-        for P in frames:
-            lib.check(L.launchRenderPipeline(ptr(f.out), ptr(f.accum), ptr(f.bloomA), ptr(f.bloomB),
+        for i, (P, fr) in enumerate(zip(frames, fs)):
+            lib.check(L.launchRenderPipeline(ptr(fr.out), ptr(fr.accum), ptr(fr.bloomA), ptr(fr.bloomB),
                                              C.byref(P), sp), "launchRenderPipeline")
-            host.copy_(f.out, non_blocking=True)
+            done = torch.cuda.Event()
+            done.record(stream)
+            cstream.wait_event(done)
+            with torch.cuda.stream(cstream):
+                hosts[i].copy_(fr.out, non_blocking=True)
+        stream.wait_stream(cstream)
         if s >= 0:
             e2[s][1].record(stream)
     torch.cuda.synchronize()
