@@ -16,8 +16,8 @@ whole job, plus frame ms.
              (bhRenderAccum + bhPostProcess per frame) is reported beside it.
   e2e        the reference-facing call: launchRenderPipeline per frame with
              RenderParams from the host, each RGBA8 frame copied back to pinned
-             host memory (on a copy stream, overlapping the next frame) inside
-             the timed region.
+             host memory, inside the timed region; frames alternate between two
+             streams, so a frame's tail and read-back overlap the next frame.
   roofline   the tracing kernel (dominant): algorithmic FLOPs / its event time
              against the measured FP32 FMA peak.  Algorithmic FLOPs follow the
              reference's work on the same inputs: RK4 steps x 420 (Kerr family)
@@ -260,21 +260,22 @@ def run_b200(args, rank, world, local_rank):
     # pinned host memory on a copy stream (overlapping the next frame's tracing); the step ends when
     # the last read-back has landed
     hosts = [torch.empty((H, W, 4), dtype=torch.uint8, pin_memory=True) for _ in range(nF)]
-    cstream = torch.cuda.Stream(device=dev)
+    side = torch.cuda.Stream(device=dev)
+    sps = (sp, C.c_void_p(side.cuda_stream))
     e2 = [(torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)) for _ in range(args.steps)]
     for s in range(-1, args.steps):
         flush.zero_()
         if s >= 0:
             e2[s][0].record(stream)
+        side.wait_stream(stream)
         for i, (P, fr) in enumerate(zip(frames, fs)):
+            # frames alternate between two streams, so one frame's tail overlaps the next frame
+            st = stream if i % 2 == 0 else side
             lib.check(L.launchRenderPipeline(ptr(fr.out), ptr(fr.accum), ptr(fr.bloomA), ptr(fr.bloomB),
-                                             C.byref(P), sp), "launchRenderPipeline")
-            done = torch.cuda.Event()
-            done.record(stream)
-            cstream.wait_event(done)
-            with torch.cuda.stream(cstream):
+                                             C.byref(P), sps[i % 2]), "launchRenderPipeline")
+            with torch.cuda.stream(st):
                 hosts[i].copy_(fr.out, non_blocking=True)
-        stream.wait_stream(cstream)
+        stream.wait_stream(side)
         if s >= 0:
             e2[s][1].record(stream)
     torch.cuda.synchronize()

@@ -10,6 +10,7 @@
 // ---------------------------------------------------------------------------
 #include <algorithm>
 #include <cmath>
+#include <atomic>
 #include <mutex>
 #include <vector>
 #include <cuda_runtime.h>
@@ -23,6 +24,25 @@ constexpr int kMaxDevices = 64;
 constexpr size_t kScratchBytes = 4096;
 std::mutex gScratchLock;
 unsigned* gScratch[kMaxDevices] = {};
+
+// Work counters: the scratch block holds a ring of kCounterSlots counters, 128 B
+// apart; every tracing launch takes the next one, so launches on different
+// streams may overlap (up to kCounterSlots in flight on a device).
+constexpr unsigned kCounterSlots = 32;
+std::atomic<unsigned> gSlot[kMaxDevices];
+
+cudaError_t deviceScratch(unsigned** out);
+
+cudaError_t launchCounter(unsigned** out)
+{
+    unsigned* base = nullptr;
+    cudaError_t e = deviceScratch(&base);
+    if (e != cudaSuccess) return e;
+    int dev = 0;
+    if ((e = cudaGetDevice(&dev)) != cudaSuccess) return e;
+    *out = base + (gSlot[dev].fetch_add(1u) % kCounterSlots) * 32u;
+    return cudaSuccess;
+}
 
 cudaError_t deviceScratch(unsigned** out)
 {
@@ -187,7 +207,7 @@ cudaError_t trace(TraceParams t, const RenderParams& P, int precision, bool stat
 {
     if (precision < BH_PREC_FP32 || precision > BH_PREC_FP64) return cudaErrorInvalidValue;
     if (!t.out) return cudaErrorInvalidValue;
-    cudaError_t e = deviceScratch(&t.counter);
+    cudaError_t e = launchCounter(&t.counter);
     if (e != cudaSuccess) return e;
     if (!t.dirs)
     {
@@ -222,7 +242,7 @@ TraceParams bh_frame_params(const RenderParams& P, int outMode, void* out)
 
 int bh_family_blocks(const RenderParams& P) { return familyBlocks(P); }
 
-cudaError_t bh_device_counter(unsigned** out) { return deviceScratch(out); }
+cudaError_t bh_device_counter(unsigned** out) { return launchCounter(out); }
 
 extern "C" {
 

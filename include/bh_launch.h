@@ -14,11 +14,12 @@
  *    (cudaGetLastError after the enqueue), as in the reference.
  *  - The caller's RenderParams is never modified: it is copied and the copy
  *    is sanitised (bhSanitizeRenderParams) before use.
- *  - Tracing kernels draw rays from a per-device work counter.  The library
- *    allocates that small scratch block (4 KiB) once per device, on the
- *    first call made on that device, and resets it on `stream` before every
- *    launch; two launches that overlap on the GPU therefore must not share
- *    a device.  Make the first call before any CUDA-graph capture begins.
+ *  - Tracing kernels draw rays from a work counter.  The library allocates a
+ *    small scratch block (4 KiB: a ring of 32 counters) once per device, on
+ *    the first call made on that device; every launch takes the next counter
+ *    of the ring and resets it on `stream`, so launches on different streams
+ *    may overlap on the GPU, up to 32 at a time per device.  Make the first
+ *    call before any CUDA-graph capture begins.
  */
 #include <cuda_runtime_api.h>
 #include <stdint.h>
@@ -191,7 +192,9 @@ typedef struct BHView
  * largest first.  FP32; CTAs per SM from bhSetTuning of each family.  The
  * library keeps per-device tables of the views' frame constants, grown on
  * demand (an allocation on the first call and when n grows; make those calls
- * outside stream capture). */
+ * outside stream capture).  Immediate-mode batches on one device share those
+ * tables, so two bhRenderBatch calls must not overlap on the GPU; the graph
+ * form below owns its own. */
 cudaError_t bhRenderBatch(const BHView* views, int n, cudaStream_t stream);
 
 /* The batch as a CUDA graph: created once for fixed views (buffers,
