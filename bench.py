@@ -80,10 +80,11 @@ def parse():
 
 
 def workload(derive, rank=0):
-    from bhrt import scenes
+    from bhrt import ranks, scenes
     frames = scenes.kerr_pair_1080(derive, W, H, FRAMES_PER_SCENE)
-    for P in frames:
-        P.diskTime = P.diskTime + float(rank)   # weak scaling: distinct frames per rank
+    times = ranks.frame_times_for_rank([P.diskTime for P in frames], rank)   # weak scaling: distinct frames
+    for P, t in zip(frames, times):
+        P.diskTime = t
     return frames
 
 
@@ -281,10 +282,9 @@ def run_b200(args, rank, world, local_rank):
     torch.cuda.synchronize()
     e2e_ms = float(sum(a.elapsed_time(b) for a, b in e2))
 
-    t = torch.tensor([total_ms, e2e_ms, batch_trace_total, pf_total], dtype=torch.float64, device=dev)
-    if world > 1:
-        dist.all_reduce(t, op=dist.ReduceOp.MAX)
-    total_ms, e2e_ms, trace_total, pf_total = t.tolist()
+    from bhrt import ranks
+    total_ms, e2e_ms, trace_total, pf_total = ranks.max_over_ranks(
+        [total_ms, e2e_ms, batch_trace_total, pf_total], world, dev)
     rays_step = nF * W * H
     out = {
         "metric": "Mrays/s (plain FP32 RK4, 1920x1080 Kerr/Kerr-Newman pair, 16 frames)",
