@@ -33,9 +33,9 @@ whole job, plus frame ms.
              random views of seed 1234 as one batch / CUDA graph vs 256
              pipeline calls.
   surrogate  (1 GPU only; --no-surrogate skips it) the learned lensing
-             surrogate: generate 16.7 M RK4-traced rays over 8192 views of the
-             batched-workload parameter box (seed 7), train 6000 Adam steps of
-             16384 rays, then 3840x2160 Kerr-Newman a*=0.8 q=0.3, r = 25,
+             surrogate: generate 64 Mi (67.1 M) RK4-traced rays over 16384 views
+             of the batched-workload parameter box (seed 7), train 24000 Adam
+             steps of 16384 rays, then 3840x2160 Kerr-Newman a*=0.8 q=0.3, r = 25,
              inclination 75 deg, FOV 45 deg frames of the 300-frame orbit: plain
              launchRenderPipeline vs bhSurrogateRender (median frame ms, pixels
              within +-1 LSB of the plain frame, RK4 share) under the strict and a
@@ -334,7 +334,7 @@ def surrogate_leg():
     h = C.c_void_p()
     lib.check(L.bhSurrogateCreate(C.byref(h), 7), "bhSurrogateCreate")
     try:
-        views, rays, steps, batch = 8192, 8192 * 2048, 6000, 16384
+        views, rays, steps, batch = 16384, 16384 * 4096, 24000, 16384   # 67 M rays (the 64 Mi of the spec)
         t0 = time.perf_counter()
         lib.check(L.bhSurrogateGenerate(h, rays, views, 7), "bhSurrogateGenerate")
         t_gen = time.perf_counter() - t0
