@@ -542,7 +542,8 @@ def main():
             peak = out["fp32_peak_tflops_measured"]
             out["roofline"] = {"bound": "fp32", "achieved": achieved, "peak": peak, "unit": "TFLOP/s",
                                "frac": achieved / peak if peak else None, "traffic": None,
-                               "peak_source": "measured FP32 FMA microbenchmark (bhMeasureFp32Peak), same run",
+                               "peak_source": "measured FP32 FMA microbenchmark, max of scalar and packed fma.rn.f32x2 "
+                                              "(bhMeasureFp32Peak), same run",
                                "flops_per_frame": flops_step / len(frames),
                                "steps_per_ray": float(np.mean([c["steps_per_ray"] for c in census]))}
             out["cpu_baseline"] = base

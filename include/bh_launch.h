@@ -248,8 +248,9 @@ cudaError_t bhAutotuneBatch(const BHView* views, int n, int* blocksKerr, int* bl
  *  - Tiles are traced in row-major order; the image is launchRenderPipeline's. */
 cudaError_t bhRenderPipelineNoAlloc(uchar4* out, float4* accum, BH_PARAMS_IN p, cudaStream_t stream);
 
-/* Measured FP32 FMA throughput of the current device, in TFLOP/s, from a
- * dependent-chain FMA kernel timed with CUDA events (blocking). */
+/* Measured FP32 FMA throughput of the current device, in TFLOP/s: the higher
+ * of a scalar-FMA and a packed FP32x2-FMA kernel (independent chains, every
+ * SM filled), timed with CUDA events (blocking). */
 double bhMeasureFp32Peak(void);
 
 /* Library version / build string. */
