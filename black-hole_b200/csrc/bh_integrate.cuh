@@ -416,44 +416,108 @@ struct KerrEval
 template <class R>
 struct KerrConsts
 {
-    R E, Lz, aE, c1, twoE;   // c1 = E a^2 - a Lz, so P = E r^2 + c1
+    R E, Lz, aE, c1, fourE;   // c1 = E a^2 - a Lz, so P = E r^2 + c1
 };
 
-template <class R>
-BH_DEV KerrEval<R> kerr_rhs(const CamFrame<R>& F, const KerrConsts<R>& k, R r, R s, R c, R pr, R pth)
+// per lane: x >= thr ? a : b
+BH_DEV float  vsel_ge(float x, float thr, float a, float b)    { return x >= thr ? a : b; }
+BH_DEV double vsel_ge(double x, double thr, double a, double b) { return x >= thr ? a : b; }
+BH_DEV float2 vsel_ge(float2 x, float2 thr, float2 a, float2 b)
 {
-    const R M = F.M, a2 = F.a2;
-    s = max_p(s, R(1e-4f));                 // pole guard
-    R r2, a2c;
-    mul2_p(r, a2, r, c, r2, a2c);
-    R Sig = r2 + a2c * c;
-    R DelRaw = r * (r - R(2) * M) + F.a2Q2;
-    R Del = max_p(DelRaw, R(1e-6f));
-    R Pp = k.E * r2 + k.c1;                 // E (r^2 + a^2) - a Lz
-    R is = rcp_p(s);
-    R iS = rcp_p(Sig);
-    R is2, iS2;
-    mul2_p(is, iS, is, iS, is2, iS2);
-    R B = k.Lz * is - k.aE * s;
-    R iDel = rcp_p(Del);
-    R PiD = Pp * iDel;
-    R W = B * B - Pp * PiD;
-    KerrEval<R> o;
-    o.K = Del * pr * pr + pth * pth + W;
-    R dDel = R(2) * (r - M);
-    R Wr = -PiD * (R(2) * k.twoE * r - PiD * dDel);   // dP = 2 r E
-    R Wth = R(-2) * B * c * (k.Lz * is2 + k.aE);
-    R mh = R(-0.5f) * iS;
-    R KiS2 = o.K * iS2;
-    mul2_p(Del * pr, pth, iS, iS, o.d.r, o.d.th);
-    o.d.ph = ((k.Lz * is2 - k.aE) + F.a * PiD) * iS;
-    R u0, u1;
-    mul2_p(r, -(a2 * s * c), KiS2, KiS2, u0, u1);
-    fma2_p(mh, dDel * pr * pr + Wr, Wth, u0, u1, o.d.pr, o.d.pth);
+    return make_float2(x.x >= thr.x ? a.x : b.x, x.y >= thr.y ? a.y : b.y);
+}
+BH_DEV void vsincos_stage(float x, float& s, float& c)    { sincos_stage(x, s, c); }
+BH_DEV void vsincos_stage(double x, double& s, double& c) { sincos_stage(x, s, c); }
+BH_DEV void vsincos_stage(float2 x, float2& s, float2& c)
+{
+    sincos_stage(x.x, s.x, c.x);
+    sincos_stage(x.y, s.y, c.y);
+}
+
+// Two updates a * x_i + y_i of one lane type with a shared coefficient: for a
+// single FP32 ray the pair is one packed FMA, otherwise two lane FMAs (the
+// same rounding either way).
+BH_DEV void vfma_pair(float a, float x0, float x1, float y0, float y1, float& o0, float& o1)
+{
+    fma2_p(a, x0, x1, y0, y1, o0, o1);
+}
+template <class V> BH_DEV void vfma_pair(V a, V x0, V x1, V y0, V y1, V& o0, V& o1)
+{
+    o0 = vfma(a, x0, y0);
+    o1 = vfma(a, x1, y1);
+}
+
+// V = float or double (one ray), float2 (two FP32 rays packed); S = the frame's
+// scalar type.  Every operation explicit, so one ray and a packed pair give the
+// same bits.
+template <class V, class S>
+BH_DEV KerrEval<V> kerr_rhs(const CamFrame<S>& F, const KerrConsts<V>& k, V r, V s, V c, V pr, V pth)
+{
+    const V M = lane<V>(F.M), a2 = lane<V>(F.a2);
+    s = vmax(s, lane<V>((S)1e-4f));                                        // pole guard
+    const V r2 = vmul(r, r);
+    const V Sig = vfma(vmul(a2, c), c, r2);                                // r^2 + a^2 cos^2
+    const V DelRaw = vfma(r, vfma(lane<V>((S)-2.f), M, r), lane<V>(F.a2Q2));   // r (r - 2M) + a^2 + Q^2
+    const V Del = vmax(DelRaw, lane<V>((S)1e-6f));
+    const V Pp = vfma(k.E, r2, k.c1);                                      // E (r^2 + a^2) - a Lz
+    const V is = vrcp(s), iS = vrcp(Sig);
+    const V is2 = vmul(is, is), iS2 = vmul(iS, iS);
+    const V B = vfma(vneg(k.aE), s, vmul(k.Lz, is));                       // Lz / s - a E s
+    const V iDel = vrcp(Del);
+    const V PiD = vmul(Pp, iDel), nPiD = vneg(PiD);
+    const V W = vfma(B, B, vmul(nPiD, Pp));                                // B^2 - P^2 / Delta
+    const V Dpr = vmul(Del, pr);
+    KerrEval<V> o;
+    o.K = vfma(Dpr, pr, vfma(pth, pth, W));                                // Delta pr^2 + pth^2 + W
+    const V dDel = vfma(lane<V>((S)-2.f), M, vadd(r, r));                  // 2 (r - M)
+    const V Wr = vmul(nPiD, vfma(nPiD, dDel, vmul(k.fourE, r)));           // -P/D (dP - P/D dDelta), dP = 2 E r
+    const V Wth = vmul(vmul(vmul(lane<V>((S)-2.f), B), c), vfma(k.Lz, is2, k.aE));   // -2 B c (Lz / s^2 + a E)
+    const V mh = vmul(lane<V>((S)-0.5f), iS);
+    const V KiS2 = vmul(o.K, iS2);
+    o.d.r = vmul(Dpr, iS);
+    o.d.th = vmul(pth, iS);
+    o.d.ph = vmul(vfma(lane<V>(F.a), PiD, vfma(k.Lz, is2, vneg(k.aE))), iS);
+    o.d.pr = vfma(mh, vfma(vmul(dDel, pr), pr, Wr), vmul(r, KiS2));
+    o.d.pth = vfma(mh, Wth, vneg(vmul(vmul(vmul(a2, s), c), KiS2)));
     o.Pp = Pp;
-    o.iDelT = (DelRaw >= R(1e-5f)) ? iDel : R(1e5f);
+    o.iDelT = vsel_ge(DelRaw, lane<V>((S)1e-5f), iDel, lane<V>((S)1e5f));
     o.iS = iS;
     return o;
+}
+
+// The classic RK4 step of the Kerr-Newman system from the state (r, th, ph,
+// pr, pth) with step h and first right-hand side d1; d4 receives the final
+// stage's derivative.  (reference src/trace.cuh:811-838)
+template <class V, class S>
+BH_DEV void kerr_rk4(const CamFrame<S>& F, const KerrConsts<V>& k, V h, V& r, V& th, V& ph, V& pr, V& pth,
+                     const KerrDeriv<V>& d1, KerrDeriv<V>& d4)
+{
+    const V hh = vmul(lane<V>((S)0.5f), h), two = lane<V>((S)2.f);
+    V sx, cx, yr, yth, ypr, ypth;
+    vfma_pair(hh, d1.r, d1.th, r, th, yr, yth);
+    vfma_pair(hh, d1.pr, d1.pth, pr, pth, ypr, ypth);
+    vsincos_stage(yth, sx, cx);
+    const KerrDeriv<V> d2 = kerr_rhs(F, k, yr, sx, cx, ypr, ypth).d;
+    V sr, sth, spr, spth, sph = vfma(two, d2.ph, d1.ph);
+    vfma_pair(two, d2.r, d2.th, d1.r, d1.th, sr, sth);
+    vfma_pair(two, d2.pr, d2.pth, d1.pr, d1.pth, spr, spth);
+    vfma_pair(hh, d2.r, d2.th, r, th, yr, yth);
+    vfma_pair(hh, d2.pr, d2.pth, pr, pth, ypr, ypth);
+    vsincos_stage(yth, sx, cx);
+    const KerrDeriv<V> d3 = kerr_rhs(F, k, yr, sx, cx, ypr, ypth).d;
+    vfma_pair(two, d3.r, d3.th, sr, sth, sr, sth);
+    vfma_pair(two, d3.pr, d3.pth, spr, spth, spr, spth);
+    sph = vfma(two, d3.ph, sph);
+    vfma_pair(h, d3.r, d3.th, r, th, yr, yth);
+    vfma_pair(h, d3.pr, d3.pth, pr, pth, ypr, ypth);
+    vsincos_stage(yth, sx, cx);
+    d4 = kerr_rhs(F, k, yr, sx, cx, ypr, ypth).d;
+    const V h6 = vmul(h, lane<V>((S)(1.0 / 6.0)));
+    V t0, t1, t2, t3;
+    t0 = vadd(sr, d4.r); t1 = vadd(sth, d4.th); t2 = vadd(spr, d4.pr); t3 = vadd(spth, d4.pth);
+    vfma_pair(h6, t0, t1, r, th, r, th);
+    vfma_pair(h6, t2, t3, pr, pth, pr, pth);
+    ph = vfma(h6, vadd(sph, d4.ph), ph);
 }
 
 // One RK4 step of the Kerr-Newman system in FP64 from an FP32 state (the
@@ -465,7 +529,7 @@ static __device__ __noinline__ KerrStep64 kerr_rk4_fp64(const CamFrame<double>& 
                                                         float th0, float ph0, float pr0, float pth0, float hf)
 {
     const double E = Ef, Lz = Lzf, h = hf;
-    const KerrConsts<double> k{E, Lz, F.a * E, E * F.a2 - F.a * Lz, 2.0 * E};
+    const KerrConsts<double> k{E, Lz, F.a * E, E * F.a2 - F.a * Lz, 4.0 * E};
     double r = r0, th = th0, ph = ph0, pr = pr0, pth = pth0, s, c;
     sincos(th, &s, &c);
     KerrDeriv<double> d1 = kerr_rhs(F, k, r, s, c, pr, pth).d;
@@ -550,7 +614,7 @@ struct KerrRay
             pth = xmul(dtc, F.sqS);
             r = F.r0; th = F.th0; ph = F.ph0;
         }
-        k.E = E; k.Lz = Lz; k.aE = F.a * E; k.c1 = E * F.a2 - F.a * Lz; k.twoE = R(2) * E;
+        k.E = E; k.Lz = Lz; k.aE = F.a * E; k.c1 = E * F.a2 - F.a * Lz; k.fourE = R(4) * E;
         sincos_theta(th, s, c);
         KerrEval<R> ev = kerr_rhs(F, k, r, s, c, pr, pth);
         d1 = ev.d;
@@ -623,35 +687,8 @@ struct KerrRay
             }
         }
 
-        // classic RK4; the (r, theta) and (p_r, p_theta) halves of every stage
-        // update are independent pairs with a shared coefficient (packed FMAs)
-        const R hh = R(0.5f) * h;
-        R sx, cx, yr, yth, ypr, ypth;
-        fma2_p(hh, d1.r, d1.th, r, th, yr, yth);
-        fma2_p(hh, d1.pr, d1.pth, pr, pth, ypr, ypth);
-        sincos_stage(yth, sx, cx);
-        KerrDeriv<R> d2 = kerr_rhs(F, k, yr, sx, cx, ypr, ypth).d;
-        R sr, sth, spr, spth, sph = d1.ph + R(2) * d2.ph;
-        fma2_p(R(2), d2.r, d2.th, d1.r, d1.th, sr, sth);
-        fma2_p(R(2), d2.pr, d2.pth, d1.pr, d1.pth, spr, spth);
-        fma2_p(hh, d2.r, d2.th, r, th, yr, yth);
-        fma2_p(hh, d2.pr, d2.pth, pr, pth, ypr, ypth);
-        sincos_stage(yth, sx, cx);
-        KerrDeriv<R> d3 = kerr_rhs(F, k, yr, sx, cx, ypr, ypth).d;
-        fma2_p(R(2), d3.r, d3.th, sr, sth, sr, sth);
-        fma2_p(R(2), d3.pr, d3.pth, spr, spth, spr, spth);
-        sph += R(2) * d3.ph;
-        fma2_p(h, d3.r, d3.th, r, th, yr, yth);
-        fma2_p(h, d3.pr, d3.pth, pr, pth, ypr, ypth);
-        sincos_stage(yth, sx, cx);
-        KerrDeriv<R> d4 = kerr_rhs(F, k, yr, sx, cx, ypr, ypth).d;
-        const R h6 = h * R(1.0 / 6.0);
-        R t0, t1, t2, t3;
-        add2_p(sr, sth, d4.r, d4.th, t0, t1);
-        add2_p(spr, spth, d4.pr, d4.pth, t2, t3);
-        fma2_p(h6, t0, t1, r, th, r, th);
-        fma2_p(h6, t2, t3, pr, pth, pr, pth);
-        ph += h6 * (sph + d4.ph);
+        KerrDeriv<R> d4;
+        kerr_rk4(F, k, h, r, th, ph, pr, pth, d1, d4);
         return finish_step(P, F, h, rS, thS, drS, dthS, d4.r, d4.th, d4.ph);
     }
 

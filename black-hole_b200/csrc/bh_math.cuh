@@ -166,6 +166,32 @@ BH_DEV void mul2_p(double x0, double x1, double y0, double y1, double& o0, doubl
     o0 = x0 * y0;
     o1 = x1 * y1;
 }
+// ---- lane arithmetic: one ray (float / double) or two rays packed (float2) ----
+// Explicit IEEE operations (no contraction decided by the compiler), so a
+// computation written once gives the same bits for a single ray and for each
+// half of a packed pair.
+BH_DEV float  vfma(float a, float b, float c)    { return __fmaf_rn(a, b, c); }
+BH_DEV double vfma(double a, double b, double c) { return fma(a, b, c); }
+BH_DEV float2 vfma(float2 a, float2 b, float2 c) { return __ffma2_rn(a, b, c); }
+BH_DEV float  vmul(float a, float b)    { return __fmul_rn(a, b); }
+BH_DEV double vmul(double a, double b)  { return __dmul_rn(a, b); }
+BH_DEV float2 vmul(float2 a, float2 b)  { return __fmul2_rn(a, b); }
+BH_DEV float  vadd(float a, float b)    { return __fadd_rn(a, b); }
+BH_DEV double vadd(double a, double b)  { return __dadd_rn(a, b); }
+BH_DEV float2 vadd(float2 a, float2 b)  { return __fadd2_rn(a, b); }
+BH_DEV float  vneg(float a)  { return -a; }
+BH_DEV double vneg(double a) { return -a; }
+BH_DEV float2 vneg(float2 a) { return make_float2(-a.x, -a.y); }
+BH_DEV float  vmax(float a, float b)    { return fmaxf(a, b); }
+BH_DEV double vmax(double a, double b)  { return fmax(a, b); }
+BH_DEV float2 vmax(float2 a, float2 b)  { return make_float2(fmaxf(a.x, b.x), fmaxf(a.y, b.y)); }
+BH_DEV float  vrcp(float a)  { return rcp_f(a); }
+BH_DEV double vrcp(double a) { return 1.0 / a; }
+BH_DEV float2 vrcp(float2 a) { return make_float2(rcp_f(a.x), rcp_f(a.y)); }
+// a per-frame scalar (float or double) in every lane of V
+template <class V, class S> BH_DEV V lane(S x) { return (V)x; }
+template <> BH_DEV float2 lane<float2, float>(float x) { return make_float2(x, x); }
+
 BH_DEV bool   finite_p(float x)  { return isfinite(x); }
 BH_DEV bool   finite_p(double x) { return isfinite(x); }
 
