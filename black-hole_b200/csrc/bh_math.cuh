@@ -58,6 +58,9 @@ BH_DEV float smoothstep_f(float e0, float e1, float x)
 // fast reciprocal: one MUFU.RCP (relative error ~2^-23)
 BH_DEV float rcp_f(float x) { float r; asm("rcp.approx.ftz.f32 %0, %1;" : "=f"(r) : "f"(x)); return r; }
 BH_DEV float rsqrt_f(float x) { float r; asm("rsqrt.approx.ftz.f32 %0, %1;" : "=f"(r) : "f"(x)); return r; }
+// MUFU base-2 logarithm and exponential (absolute error ~2^-22 near 1, subnormals flushed)
+BH_DEV float lg2_f(float x) { float r; asm("lg2.approx.ftz.f32 %0, %1;" : "=f"(r) : "f"(x)); return r; }
+BH_DEV float ex2_f(float x) { float r; asm("ex2.approx.ftz.f32 %0, %1;" : "=f"(r) : "f"(x)); return r; }
 // fast square root (MUFU based, relative error ~2^-22, sqrt(0) = 0)
 BH_DEV float sqrt_a(float x) { float r; asm("sqrt.approx.f32 %0, %1;" : "=f"(r) : "f"(x)); return r; }
 

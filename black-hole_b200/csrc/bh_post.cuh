@@ -22,6 +22,23 @@ BH_DEV f3 aces_x(f3 x)
     return v3(one(x.x), one(x.y), one(x.z));
 }
 
+// Gamma 1/2.2, dither and 8-bit quantisation of one channel x in [0, 1]:
+// byte = trunc(clamp(x^(1/2.2) + dd, 0, 1) * 255 + 0.5), the power being the
+// full-accuracy powf.  The MUFU form exp2(log2(x) / 2.2) (relative error
+// below 1e-6, i.e. below 3e-4 in units of the unrounded byte value y) decides
+// the byte wherever y lies more than 1e-3 from a truncation boundary; within
+// that margin powf recomputes it.  The byte is therefore always the one powf
+// gives, at a fraction of its cost (powf was a third of the tonemap's work).
+BH_DEV unsigned char gamma_q8(float x, float dd)
+{
+    const float g = 1.0f / 2.2f;
+    float y = add_x(mul_x(clampf(add_x(ex2_f(mul_x(lg2_f(x), g)), dd), 0.f, 1.f), 255.f), 0.5f);
+    const float fr = sub_x(y, floorf(y));
+    if (fr < 1e-3f || fr > 0.999f)
+        y = add_x(mul_x(clampf(add_x(powf(x, g), dd), 0.f, 1.f), 255.f), 0.5f);
+    return (unsigned char)__float2uint_rz(y);
+}
+
 // exposure -> bloom composite -> ACES -> vibrance 1.12 -> gamma 1/2.2 -> dither -> u8
 BH_DEV uchar4 finalize_pixel(f3 hdr, f3 bloom, const PostConsts& pc, int px, int py)
 {
@@ -34,15 +51,10 @@ BH_DEV uchar4 finalize_pixel(f3 hdr, f3 bloom, const PostConsts& pc, int px, int
     c = v3(clampf(add_x(lum, mul_x(sub_x(c.x, lum), 1.12f)), 0.f, 1.f),
            clampf(add_x(lum, mul_x(sub_x(c.y, lum), 1.12f)), 0.f, 1.f),
            clampf(add_x(lum, mul_x(sub_x(c.z, lum), 1.12f)), 0.f, 1.f));
-    const float g = 1.0f / 2.2f;
-    c = v3(powf(c.x, g), powf(c.y, g), powf(c.z, g));
     float fx = (float)px, fy = (float)py;
     float d = sub_x(add_x(hash12(fx, fy), hash12(add_x(fx, 41.3f), add_x(fy, 17.7f))), 1.0f);
     float dd = mul_x(d, 1.0f / 255.0f);
-    auto q8 = [&](float v) {
-        return (unsigned char)__float2uint_rz(add_x(mul_x(clampf(add_x(v, dd), 0.f, 1.f), 255.f), 0.5f));
-    };
-    unsigned char r8 = q8(c.x), g8 = q8(c.y), b8 = q8(c.z);
+    unsigned char r8 = gamma_q8(c.x, dd), g8 = gamma_q8(c.y, dd), b8 = gamma_q8(c.z, dd);
     return pc.swapRB ? make_uchar4(b8, g8, r8, 255) : make_uchar4(r8, g8, b8, 255);
 }
 
