@@ -32,6 +32,10 @@ whole job, plus frame ms.
              3840x2160 near-extremal Kerr-Newman elevation sweep, and the 256
              random views of seed 1234 as one batch / CUDA graph vs 256
              pipeline calls.
+  post_process  (1 GPU only; --no-configs skips it) bloom + tonemap on a
+             rendered 3840x2160 frame: microseconds per frame and achieved HBM
+             GB/s (28 B per pixel, the fused-minimum traffic) against the
+             measured HBM peak, with bloom on and off.
   surrogate  (1 GPU only; --no-surrogate skips it) the learned lensing
              surrogate: generate 64 Mi (67.1 M) RK4-traced rays over 16384 views
              of the batched-workload parameter box (seed 7), train 24000 Adam
@@ -464,6 +468,52 @@ def mixed_leg():
     return res
 
 
+def post_leg():
+    """Bloom + tonemap (bloom_h_kernel + composite_kernel through bhPostProcess) on a rendered
+    3840x2160 accumulation buffer (frame 60 of the Kerr-Newman a*=0.998 sweep): 133 MB of float4,
+    larger than L2, and L2 flushed before every launch.  Achieved HBM GB/s uses the fused-minimum
+    algorithmic traffic of 28 B per full-resolution pixel (16 B accumulation read, 4 B RGBA8 write,
+    ~8 B half-resolution bloom)."""
+    import torch
+    from bhrt import lib, scenes
+    from bhrt.device import Frame
+    P = scenes.kn_sweep_4k(lib.derive, 3840, 2160, frames=120, frame_ids=(60,))[0]
+    f = Frame(3840, 2160)
+    f.pipeline(P)
+    flush = torch.empty(L2_FLUSH_BYTES, dtype=torch.uint8, device="cuda")
+    e0, e1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+    peaks = {}
+    try:
+        with open(os.path.join(ROOT, "MEASURED_PEAKS.json")) as fh:
+            peaks = json.load(fh)
+    except (OSError, ValueError):
+        pass
+    hbm = peaks.get("hbm_gbs", 6650.0)
+    res = {"workload": "bhPostProcess on kn_a0.998_q0.05_r12_fov50_3840x2160 frame 60 (accum 133 MB > L2, "
+                       "L2 flushed per launch)",
+           "kernels": ["bloom_h_kernel", "composite_kernel"], "algorithmic_bytes_per_px": 28.0,
+           "peak_gbs": hbm, "peak_source": "MEASURED_PEAKS.json hbm_gbs" if peaks else "fallback"}
+    npx = 3840 * 2160
+    for bloom in (1, 0):
+        P.bloomEnabled = bloom
+        for _ in range(3):
+            f.post(P)
+        ts = []
+        for _ in range(20):
+            flush.zero_()
+            e0.record()
+            f.post(P)
+            e1.record()
+            torch.cuda.synchronize()
+            ts.append(e0.elapsed_time(e1))
+        us = float(np.median(ts)) * 1e3
+        byts = (28.0 if bloom else 20.0) * npx
+        key = "bloom_on" if bloom else "bloom_off"
+        res[key] = {"us_per_frame": us, "achieved_gbs": byts / (us * 1e-6) / 1e9,
+                    "frac": byts / (us * 1e-6) / 1e9 / hbm}
+    return res
+
+
 def batch256_leg():
     """The 256 random views of seed 1234 (all four families, 128x72 .. 1920x1080): one bhRenderBatch
     call vs 256 launchRenderPipeline calls, and the CUDA-graph replay."""
@@ -550,6 +600,7 @@ def main():
         if world == 1 and not args.no_configs:
             out["mixed_precision_4k"] = mixed_leg()
             out["batch_256_views"] = batch256_leg()
+            out["post_process"] = post_leg()
         if world == 1 and not args.no_surrogate:
             out["surrogate"] = surrogate_leg()
         print(json.dumps(out))

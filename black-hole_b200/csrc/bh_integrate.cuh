@@ -22,13 +22,13 @@
 // accuracy oracle).  Shading stays float in both.
 //
 // Arithmetic of the FP32 step: divisions by state-dependent quantities use one
-// MUFU reciprocal each; sin/cos of the polar angle at the start of a step come
-// from the polynomial sincos_polar (relative accuracy at poles and equator)
-// and are carried into the next step's first right-hand side, the slow-light
-// term and the Cartesian chord; the three RK4 stage angles th + delta use the
-// angle-addition formula from that anchored pair; the ever-growing azimuth
-// uses sincos_fast.  The escape direction is rebuilt once per ray with the
-// accurate library sincos.
+// MUFU reciprocal each; sin/cos of the polar angle (at the start of a step and
+// at the three RK4 stage angles) use the MUFU pair, replaced by the polynomial
+// sincos_polar where |sin| < 1/16 so the pole terms keep relative accuracy; the
+// pair at the start of a step is carried into the next step's first
+// right-hand side, the slow-light term and the Cartesian chord; the
+// ever-growing azimuth uses sincos_fast.  The escape direction is rebuilt once
+// per ray with the accurate library sincos.
 // ---------------------------------------------------------------------------
 #include <type_traits>
 #include "bh_shade.cuh"
