@@ -457,28 +457,28 @@ BH_DEV KerrEval<V> kerr_rhs(const CamFrame<S>& F, const KerrConsts<V>& k, V r, V
     s = vmax(s, lane<V>((S)1e-4f));                                        // pole guard
     const V r2 = vmul(r, r);
     const V Sig = vfma(vmul(a2, c), c, r2);                                // r^2 + a^2 cos^2
-    const V DelRaw = vfma(r, vfma(lane<V>((S)-2.f), M, r), lane<V>(F.a2Q2));   // r (r - 2M) + a^2 + Q^2
+    const V rm2M = vfma(lane<V>((S)-2.f), M, r);                           // r - 2M
+    const V DelRaw = vfma(r, rm2M, lane<V>(F.a2Q2));                       // r (r - 2M) + a^2 + Q^2
     const V Del = vmax(DelRaw, lane<V>((S)1e-6f));
     const V Pp = vfma(k.E, r2, k.c1);                                      // E (r^2 + a^2) - a Lz
-    const V is = vrcp(s), iS = vrcp(Sig);
-    const V is2 = vmul(is, is), iS2 = vmul(iS, iS);
+    const V is = vrcp(s), iS = vrcp(Sig), iDel = vrcp(Del);
+    const V is2 = vmul(is, is);
     const V B = vfma(vneg(k.aE), s, vmul(k.Lz, is));                       // Lz / s - a E s
-    const V iDel = vrcp(Del);
-    const V PiD = vmul(Pp, iDel), nPiD = vneg(PiD);
-    const V W = vfma(B, B, vmul(nPiD, Pp));                                // B^2 - P^2 / Delta
+    const V PiD = vmul(Pp, iDel);
+    const V W = vfma(B, B, vneg(vmul(PiD, Pp)));                           // B^2 - P^2 / Delta
     const V Dpr = vmul(Del, pr);
     KerrEval<V> o;
     o.K = vfma(Dpr, pr, vfma(pth, pth, W));                                // Delta pr^2 + pth^2 + W
-    const V dDel = vfma(lane<V>((S)-2.f), M, vadd(r, r));                  // 2 (r - M)
-    const V Wr = vmul(nPiD, vfma(nPiD, dDel, vmul(k.fourE, r)));           // -P/D (dP - P/D dDelta), dP = 2 E r
-    const V Wth = vmul(vmul(vmul(lane<V>((S)-2.f), B), c), vfma(k.Lz, is2, k.aE));   // -2 B c (Lz / s^2 + a E)
-    const V mh = vmul(lane<V>((S)-0.5f), iS);
-    const V KiS2 = vmul(o.K, iS2);
+    const V dDel = vadd(rm2M, r);                                          // dDelta/dr = 2 (r - M)
+    const V Wr = vmul(PiD, vfma(PiD, dDel, vneg(vmul(k.fourE, r))));       // dW/dr = -P/D (dP - P/D dDelta)
+    const V KiS = vmul(o.K, iS);
     o.d.r = vmul(Dpr, iS);
     o.d.th = vmul(pth, iS);
     o.d.ph = vmul(vfma(lane<V>(F.a), PiD, vfma(k.Lz, is2, vneg(k.aE))), iS);
-    o.d.pr = vfma(mh, vfma(vmul(dDel, pr), pr, Wr), vmul(r, KiS2));
-    o.d.pth = vfma(mh, Wth, vneg(vmul(vmul(vmul(a2, s), c), KiS2)));
+    // dpr = -(dH/dr) = (r K / Sigma - (dDelta pr^2 + dW/dr) / 2) / Sigma
+    o.d.pr = vmul(iS, vfma(lane<V>((S)-0.5f), vfma(vmul(dDel, pr), pr, Wr), vmul(r, KiS)));
+    // dpth = -(dH/dth) = cos (B (Lz / s^2 + a E) - a^2 s K / Sigma) / Sigma
+    o.d.pth = vmul(vmul(c, iS), vfma(B, vfma(k.Lz, is2, k.aE), vneg(vmul(vmul(a2, s), KiS))));
     o.Pp = Pp;
     o.iDelT = vsel_ge(DelRaw, lane<V>((S)1e-5f), iDel, lane<V>((S)1e5f));
     o.iS = iS;
