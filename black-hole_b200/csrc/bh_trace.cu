@@ -252,11 +252,11 @@ trace_kernel(const __grid_constant__ TraceParams P)
 // One tile (32 rays) of one view, traced by a whole warp: tile-synchronous, the
 // warp shades its 32 results together once every lane is done.
 template <class Ray>
-BH_DEV void trace_tile(const TraceParams& P, unsigned tile, unsigned lane)
+BH_DEV void trace_tile(const TraceParams& P, unsigned tile, unsigned lane, unsigned nRays)
 {
     const unsigned rid = tile * 32u + lane;
     int px = 0, py = 0;
-    const bool inFrame = ray_pixel(P, rid, px, py);
+    const bool inFrame = rid < nRays && ray_pixel(P, rid, px, py);
     Ray ray;
     bool live = false, fin = false;
     unsigned key = 0;
@@ -275,6 +275,31 @@ BH_DEV void trace_tile(const TraceParams& P, unsigned tile, unsigned lane)
         PackedRay<typename Ray::Real> q;
         ray.pack(P, key, q, nullptr);
         shade_slot<Ray, false>(P, q, nullptr);
+    }
+}
+
+// One frame (or one pixel list), tile-synchronous: each warp claims 32 ray
+// ids -- one 8x4 tile, or 32 consecutive list entries -- at a time (the
+// counter counts tiles) and traces them to the last ray.  This is the FP32
+// render path under the default work distribution (a warp refills only when
+// all 32 lanes are idle); it skips trace_kernel's per-step ballots and result
+// ring.  Plain frames and the surrogate's RK4 pixel lists share this kernel,
+// so a pixel traced by either gets the same bits.
+template <class Ray>
+__global__ void __launch_bounds__(BH_TRACE_BLOCK, min_blocks<Ray, false>())
+tile_kernel(const __grid_constant__ TraceParams P)
+{
+    const unsigned lane = threadIdx.x & 31u;
+    const unsigned nRays = P.nRaysDev ? *P.nRaysDev : P.nRays;
+    const unsigned nTiles = (nRays + 31u) / 32u;
+    while (true)
+    {
+        unsigned t = 0;
+        if (lane == 0) t = atomicAdd(P.counter, 1u);
+        t = __shfl_sync(0xffffffffu, t, 0);
+        if (t >= nTiles) break;
+        trace_tile<Ray>(P, t, lane, nRays);
+        __syncwarp();
     }
 }
 
@@ -311,7 +336,7 @@ batch_kernel(const TraceParams* __restrict__ views, const unsigned* __restrict__
             __syncwarp();
             cur = lo;
         }
-        trace_tile<Ray>(sp[warp], g - __ldg(tileBase + lo), lane);
+        trace_tile<Ray>(sp[warp], g - __ldg(tileBase + lo), lane, sp[warp].nRays);
         __syncwarp();
     }
 }
@@ -321,6 +346,10 @@ template <class Ray, bool STATS>
 cudaError_t launch_one(const TraceParams& P, int blocksPerSm, cudaStream_t stream)
 {
     auto k = trace_kernel<Ray, STATS>;
+    if constexpr (!STATS && sizeof(typename Ray::Real) == 4)
+    {   // whole frames under the default work distribution: tile-synchronous
+        if (P.refillMin >= 32 && !P.dirs) k = tile_kernel<Ray>;
+    }
     int dev = 0, sms = 0, occ = 0;
     cudaError_t e = cudaGetDevice(&dev);
     if (e != cudaSuccess) return e;
