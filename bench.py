@@ -96,43 +96,66 @@ def workload(derive, rank=0):
 # clocks during the timed region
 # ---------------------------------------------------------------------------
 class ClockSampler:
-    Q = ("clocks.sm,clocks.max.sm,power.draw,clocks_event_reasons.hw_slowdown,"
+    """nvidia-smi clock / throttle samples every 50 ms.  Started before the warm-up (nvidia-smi takes a
+    few hundred ms to start); only the samples whose own timestamps fall inside the timed window
+    (mark_start .. mark_stop, host wall clock) are reported."""
+    Q = ("timestamp,clocks.sm,clocks.max.sm,power.draw,clocks_event_reasons.hw_slowdown,"
          "clocks_event_reasons.hw_thermal_slowdown,clocks_event_reasons.sw_thermal_slowdown,"
          "clocks_event_reasons.sw_power_cap")
 
     def __init__(self, index):
         self.index, self.rows, self.proc = index, [], None
+        self.t0 = self.t1 = None
 
     def start(self):
         try:
             self.proc = subprocess.Popen(["nvidia-smi", "-i", str(self.index), f"--query-gpu={self.Q}",
-                                          "--format=csv,noheader,nounits", "-lms", "200"],
+                                          "--format=csv,noheader,nounits", "-lms", "50"],
                                          stdout=subprocess.PIPE, stderr=subprocess.DEVNULL, text=True)
             self.thread = threading.Thread(target=self._read, daemon=True)
             self.thread.start()
         except OSError:
             self.proc = None
 
+    def mark_start(self):
+        self.t0 = time.time()
+
+    def mark_stop(self):
+        self.t1 = time.time()
+
     def _read(self):
         for line in self.proc.stdout:
             parts = [p.strip() for p in line.split(",")]
-            if len(parts) == 7:
+            if len(parts) == 8:
                 self.rows.append(parts)
+
+    @staticmethod
+    def _when(stamp):
+        from datetime import datetime
+        try:
+            return datetime.strptime(stamp, "%Y/%m/%d %H:%M:%S.%f").timestamp()
+        except ValueError:
+            return None
 
     def stop(self):
         if self.proc is None:
             return {"sm_mhz": None, "sm_max_mhz": None, "reasons": ["nvidia-smi unavailable"]}
+        time.sleep(0.2)    # let the samples of the window's last 50 ms arrive
         self.proc.terminate()
         try:
             self.proc.wait(timeout=5)
         except subprocess.TimeoutExpired:
             self.proc.kill()
-        sm = [float(r[0]) for r in self.rows if r[0].replace(".", "").isdigit()]
-        mx = [float(r[1]) for r in self.rows if r[1].replace(".", "").isdigit()]
+        rows = self.rows
+        if self.t0 is not None and self.t1 is not None:
+            inside = [r for r in rows if (w := self._when(r[0])) is not None and self.t0 <= w <= self.t1]
+            rows = inside or rows[-1:]
+        sm = [float(r[1]) for r in rows if r[1].replace(".", "").isdigit()]
+        mx = [float(r[2]) for r in rows if r[2].replace(".", "").isdigit()]
         names = ["hw_slowdown", "hw_thermal_slowdown", "sw_thermal_slowdown", "sw_power_cap"]
-        reasons = sorted({names[i] for r in self.rows for i in range(4) if r[3 + i] == "Active"})
+        reasons = sorted({names[i] for r in rows for i in range(4) if r[4 + i] == "Active"})
         return {"sm_mhz": float(np.median(sm)) if sm else None, "sm_max_mhz": max(mx) if mx else None,
-                "reasons": reasons, "samples": len(self.rows)}
+                "reasons": reasons, "samples": len(rows)}
 
 
 # ---------------------------------------------------------------------------
@@ -226,23 +249,25 @@ def run_b200(args, rank, world, local_rank):
             if evs is not None:
                 evs[i][2].record(stream)
 
+    clocks = ClockSampler(local_rank)
+    clocks.start()
     for _ in range(args.warmup):
         batch()
         per_frame()
     torch.cuda.synchronize()
 
     ev = [(torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)) for _ in range(args.steps)]
-    clocks = ClockSampler(local_rank)
     if world > 1:
         dist.barrier()
     torch.cuda.synchronize()
-    clocks.start()
+    clocks.mark_start()
     for s in range(args.steps):
         flush.zero_()
         ev[s][0].record(stream)
         batch()
         ev[s][1].record(stream)
     torch.cuda.synchronize()
+    clocks.mark_stop()
     if world > 1:
         dist.barrier()
     clk = clocks.stop()
