@@ -148,3 +148,24 @@ def test_batch_autotune_then_batch_still_matches(cuda):
     finally:
         lib.set_tuning(0, *before[0])
         lib.set_tuning(1, *before[1])
+
+
+def test_refill_kernel_agrees_with_tile_kernel(cuda):
+    """Under the default work distribution frames run the tile-synchronous
+    kernel; with refillMin < 32 they run the refill-queue kernel.  Both trace
+    every ray with the same step loop, so the frames agree to rounding (the two
+    kernels are compiled separately and may contract a multiply-add
+    differently): every pixel within +-1 LSB but a handful."""
+    params = _views(12, seed=7)
+    tile = _singles(params)
+    before = lib.get_tuning(0), lib.get_tuning(1)
+    try:
+        lib.set_tuning(0, 16, before[0][1])
+        lib.set_tuning(1, 16, before[1][1])
+        refill = _singles(params)
+    finally:
+        lib.set_tuning(0, *before[0])
+        lib.set_tuning(1, *before[1])
+    for a, b in zip(refill, tile):
+        s = parity.compare_rgba(a, b)
+        assert s["alpha_ok"] and s["lsb1_frac"] >= 0.9995 and s["exact_frac"] >= 0.99, s
