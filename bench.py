@@ -32,6 +32,11 @@ whole job, plus frame ms.
              3840x2160 near-extremal Kerr-Newman elevation sweep, and the 256
              random views of seed 1234 as one batch / CUDA graph vs 256
              pipeline calls.
+  accuracy   (1 GPU only; --no-configs skips it) the plain FP32 integration of
+             the two bench scenes at 480x270 against the FP64 small-step
+             integration (dPhi/16, 16x budget): class mismatches off class
+             boundaries, escape-direction and HDR error, and the drift of the
+             Carter constant and the null Hamiltonian along the FP32 rays.
   post_process  (1 GPU only; --no-configs skips it) bloom + tonemap on a
              rendered 3840x2160 frame: microseconds per frame and achieved HBM
              GB/s (28 B per pixel, the fused-minimum traffic) against the
@@ -493,6 +498,71 @@ def mixed_leg():
     return res
 
 
+def _class_edge(cls):
+    """True where the 3x3 pixel neighbourhood (clamped) holds more than one class."""
+    c = np.asarray(cls)
+    p = np.pad(c, 1, mode="edge")
+    edge = np.zeros(c.shape, dtype=bool)
+    for dy in (0, 1, 2):
+        for dx in (0, 1, 2):
+            edge |= p[dy:dy + c.shape[0], dx:dx + c.shape[1]] != c
+    return edge
+
+
+def _ray_errors(x, ref):
+    """Statistics of probe records x against ref (same grid): class mismatches off class boundaries,
+    escape-direction angle (from the difference vector in float64, resolving ~1e-7 rad) and HDR
+    relative error on rays off the boundary."""
+    inner = ~_class_edge(ref["cls"])
+    esc = inner & (x["cls"] == 2) & (ref["cls"] == 2)
+    d = x["escDir"][esc].astype(np.float64) - ref["escDir"][esc].astype(np.float64)
+    ang = 2.0 * np.arcsin(np.minimum(1.0, np.sqrt((d * d).sum(-1)) / 2.0))
+    hx, hr = x["hdr"][inner].astype(np.float64), ref["hdr"][inner].astype(np.float64)
+    hrel = (np.abs(hx - hr) / np.maximum(np.abs(hr), 1e-3)).max(-1)
+    return {"class_mismatch_off_boundary": int(((x["cls"] != ref["cls"]) & inner).sum()),
+            "rays_off_boundary": int(inner.sum()),
+            "escape_dir_err_rad": {"median": float(np.median(ang)), "p99": float(np.quantile(ang, 0.99)),
+                                   "frac_within_1e-4": float((ang <= 1e-4).mean())},
+            "hdr_rel_err": {"median": float(np.median(hrel)), "frac_within_1e-3": float((hrel <= 1e-3).mean())}}
+
+
+def accuracy_leg():
+    """The plain FP32 integration against the FP64 small-step integration (dPhi / 16, 16x the step
+    budget; the library's own FP64 kernel) of the bench's two scenes at 480x270, frame 0 of each,
+    per-ray records from bhProbeGrid.  FP64 at the FP32 step size against the same small-step run
+    separates the method's truncation error from FP32 rounding.  Conserved quantities along the FP32
+    rays: E and L_z are constants of both integrators' equations, so only the Carter constant (Binet
+    first integral) and the null Hamiltonian can drift."""
+    from bhrt import lib, scenes
+    from bhrt.abi import BH_PREC_FP32, BH_PREC_FP64
+    from bhrt.device import probe_grid
+    nx, ny = 480, 270
+    frames = scenes.kerr_pair_1080(lib.derive, nx, ny, FRAMES_PER_SCENE)
+    res = {"workload": "kerr_a0.9 and kn_a-0.7_q0.4 frame 0 at 480x270 (disk, hot spots on); reference: "
+                       "FP64 with dPhi/16 and 16x maxSteps; all on the GPU",
+           "off_boundary": "rays whose reference 3x3 pixel neighbourhood holds one class"}
+    for name, P in (("kerr_a0.9", frames[0]), ("kn_a-0.7_q0.4", frames[FRAMES_PER_SCENE])):
+        a = probe_grid(P, nx, ny, BH_PREC_FP32)
+        c = probe_grid(P, nx, ny, BH_PREC_FP64)
+        Q = P.copy()
+        Q.dPhi, Q.maxSteps = P.dPhi / 16.0, P.maxSteps * 16
+        b = probe_grid(Q, nx, ny, BH_PREC_FP64)
+        live = a["cls"] != 0
+        res[name] = {
+            "fp32_vs_small_step": _ray_errors(a, b),
+            "fp64_same_step_vs_small_step": _ray_errors(c, b),
+            "fp32_drift": {"carter_q_rel_median": float(np.median(a["drift"][live])),
+                           "carter_q_rel_max": float(a["drift"][live].max()),
+                           "null_hamiltonian_median": float(np.median(a["maxHviol"][live])),
+                           "null_hamiltonian_max": float(a["maxHviol"][live].max()),
+                           "energy_and_lz": "exact (constants of the integrated equations)"},
+            "fp64_same_step_drift": {"carter_q_rel_median": float(np.median(c["drift"][c["cls"] != 0])),
+                                     "null_hamiltonian_median": float(np.median(c["maxHviol"][c["cls"] != 0]))},
+            "steps_per_ray": {"fp32": float(a["steps"].mean()), "fp64_small_step": float(b["steps"].mean())},
+        }
+    return res
+
+
 def post_leg():
     """Bloom + tonemap (bloom_h_kernel + composite_kernel through bhPostProcess) on a rendered
     3840x2160 accumulation buffer (frame 60 of the Kerr-Newman a*=0.998 sweep): 133 MB of float4,
@@ -626,6 +696,7 @@ def main():
             out["mixed_precision_4k"] = mixed_leg()
             out["batch_256_views"] = batch256_leg()
             out["post_process"] = post_leg()
+            out["accuracy"] = accuracy_leg()
         if world == 1 and not args.no_surrogate:
             out["surrogate"] = surrogate_leg()
         print(json.dumps(out))
