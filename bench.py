@@ -495,6 +495,18 @@ def mixed_leg():
                      "frame_ms_by_elevation_deg": {str(round(89.0 * k / 119, 1)): m for k, m in zip(ids, ms)}}
     res["workload"] = "kn_a0.998_q0.05_r12_fov50_3840x2160_sweep (frames 0, 30, 60, 90, 119 of 120)"
     res["mixed_over_fp32_time"] = res["mixed"]["frame_ms"] / res["fp32"]["frame_ms"]
+    # accuracy: FP32 and mixed against the all-FP64 integration (same step control) of the same
+    # frames, per-ray records on a 480x270 grid of each camera
+    from bhrt.abi import BH_PREC_FP64
+    from bhrt.device import probe_grid
+    acc = {}
+    for k, P in zip(ids, frames):
+        ref = probe_grid(P, 480, 270, BH_PREC_FP64)
+        acc[str(round(89.0 * k / 119, 1))] = {
+            "fp32": _ray_errors(probe_grid(P, 480, 270, BH_PREC_FP32), ref),
+            "mixed": _ray_errors(probe_grid(P, 480, 270, BH_PREC_MIXED), ref)}
+    res["accuracy_vs_fp64_by_elevation_deg"] = acc
+    res["accuracy_grid"] = "480x270 per frame, reference: the all-FP64 GPU integration"
     return res
 
 
