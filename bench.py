@@ -2,58 +2,51 @@
 
     python bench.py [--gpus N] [--steps K] [--warmup W] [--impl b200|reference]
 
-Workload (one step): the 1920x1080 Kerr a*=+0.9 and Kerr-Newman a*=-0.7 q=0.4
-pair, camera r = 20, inclination 80 deg, FOV 45 deg, disk + hot spots, bloom +
-tonemap, 8 frames each with diskTime = k/7: 16 full frames, plain FP32 RK4,
-balanced preset.  Metric: Mrays/s (one primary ray per pixel) over the
-whole job, plus frame ms.
+Workload (the configuration the headline metric is quoted on): 3840x2160
+Kerr-Newman a*=0.8 q=0.3, camera r = 25, inclination 75 deg, FOV 45 deg, disk
++ hot spots, bloom + tonemap, balanced preset, plain FP32 RK4.  A step is 30
+frames of the 300-frame camera orbit (azimuth 360 k / 300 deg, every 10th
+frame; rank r of a multi-GPU run takes the frames offset by r).  Metric:
+Mrays/s (one primary ray per pixel) over the whole job, and 4K frame ms.
 
-  value      device-resident throughput: per step an L2 flush (256 MiB memset,
-             outside the timed events), then the 16 frames through
-             bhRenderBatch (one persistent tracing launch over all 16 frames'
-             tiles, then each frame's bloom + tonemap), timed with CUDA events
-             on the launch stream; max over ranks.  The per-frame form
-             (bhRenderAccum + bhPostProcess per frame) is reported beside it.
-  e2e        the reference-facing call: launchRenderPipeline per frame with
-             RenderParams from the host, each RGBA8 frame copied back to pinned
-             host memory, inside the timed region; frames alternate between two
-             streams, so a frame's tail and read-back overlap the next frame.
+  value      device-resident throughput of the reference-facing pipeline: per
+             step an L2 flush (256 MiB memset, outside the timed events), then
+             per frame bhRenderAccum + bhPostProcess (together exactly
+             launchRenderPipeline) with CUDA events around each, on the launch
+             stream; max over ranks.  frame_ms = median frame time.
+  e2e        launchRenderPipeline per frame with RenderParams from the host,
+             each RGBA8 frame copied back to pinned host memory, inside the
+             timed region; frames alternate between two streams, so a frame's
+             tail and read-back overlap the next frame.
   roofline   the tracing kernel (dominant): algorithmic FLOPs / its event time
-             against the measured FP32 FMA peak.  Algorithmic FLOPs follow the
-             reference's work on the same inputs: RK4 steps x 420 (Kerr family)
-             or x 115 (spherical), + 500 per contributing disk sub-sample
-             + 250 per escaped ray, counted by the CPU oracle on a pixel sample
-             of every frame (the census in the CPU-baseline leg).
+             (the bhRenderAccum intervals of the timed steps) against the FP32
+             FMA peak measured in the same run.  Algorithmic FLOPs follow the
+             reference's work on the same inputs: RK4 steps x 420 (Kerr
+             family) or x 115 (spherical), + 500 per contributing disk
+             sub-sample + 250 per escaped ray, counted by the CPU oracle on a
+             1/24^2 pixel sample of every frame.
   cpu_baseline  the reference's own tracer (src/trace.cuh built as host code,
-             oracle/_ref) on the host cores, on a bounded pixel sample.
+             oracle/_ref) on all host cores, on a bounded pixel sample.
+  reference_gpu_kernel  the reference's own black_hole_kernel.cu built
+             unchanged for sm_100a (oracle/_ref/libbhref_gpu.so, its
+             launchRenderPipeline) on the same 30 frames and buffers, CUDA
+             events, L2 flushed: frame ms and this build's speed-up over it.
+  surrogate  (1 GPU; --no-surrogate skips it) the learned lensing surrogate
+             on the same scene: training from RK4-traced rays, then
+             bhSurrogateRender vs the plain frame under the strict acceptance
+             gate (and a permissive one), pixels within +-1 LSB.
+  mixed_precision_4k, batch_256_views, post_process, accuracy, kerr_pair_1080
+             (1 GPU; --no-configs skips them) the other workloads: the
+             near-extremal 4K elevation sweep (FP32 vs mixed precision, frame
+             ms and accuracy against the FP64 integration), the 256 random
+             views of seed 1234 (one batch / CUDA graph vs 256 calls), bloom +
+             tonemap HBM throughput at 4K, FP32 against the FP64 small-step
+             integration with conserved-quantity drift, and the 1920x1080
+             Kerr / Kerr-Newman pair through bhRenderBatch.
 
-  mixed_precision_4k, batch_256_views  (1 GPU only; --no-configs skips them)
-             frame ms of plain FP32 vs the mixed-precision mode on the
-             3840x2160 near-extremal Kerr-Newman elevation sweep, and the 256
-             random views of seed 1234 as one batch / CUDA graph vs 256
-             pipeline calls.
-  accuracy   (1 GPU only; --no-configs skips it) the plain FP32 integration of
-             the two bench scenes at 480x270 against the FP64 small-step
-             integration (dPhi/16, 16x budget): class mismatches off class
-             boundaries, escape-direction and HDR error, and the drift of the
-             Carter constant and the null Hamiltonian along the FP32 rays.
-  post_process  (1 GPU only; --no-configs skips it) bloom + tonemap on a
-             rendered 3840x2160 frame: microseconds per frame and achieved HBM
-             GB/s (28 B per pixel, the fused-minimum traffic) against the
-             measured HBM peak, with bloom on and off.
-  surrogate  (1 GPU only; --no-surrogate skips it) the learned lensing
-             surrogate: generate 64 Mi (67.1 M) RK4-traced rays over 16384 views
-             of the batched-workload parameter box (seed 7), train 24000 Adam
-             steps of 16384 rays, then 3840x2160 Kerr-Newman a*=0.8 q=0.3, r = 25,
-             inclination 75 deg, FOV 45 deg frames of the 300-frame orbit: plain
-             launchRenderPipeline vs bhSurrogateRender (median frame ms, pixels
-             within +-1 LSB of the plain frame, RK4 share) under the strict and a
-             permissive acceptance gate; fused tensor-core MLP throughput against
-             the measured BF16 peak.
-
-Multi-GPU: one process per GPU (torchrun); every rank renders its own 16-frame
-batch (frames offset in animation time), no collective on the data path
-("scaling": "weak"); timing is the max over ranks.
+Multi-GPU: one process per GPU (torchrun); every rank renders its own 30
+frames (no collective on the data path, "scaling": "weak"); timing is the max
+over ranks.
 """
 import argparse
 import json
@@ -69,10 +62,17 @@ ROOT = os.path.dirname(os.path.abspath(__file__))
 sys.path.insert(0, os.path.join(ROOT, "black-hole_b200"))
 
 C_STEP_KERR, C_STEP_SPH, C_DISK, C_BG = 420.0, 115.0, 500.0, 250.0
-FRAMES_PER_SCENE = 8
-W, H = 1920, 1080
+W, H = 3840, 2160
+ORBIT_FRAMES, FRAMES_PER_STEP = 300, 30
 L2_FLUSH_BYTES = 256 << 20
-RAY_BYTES = 160   # RenderParams per frame, passed by value to the launch
+PARAM_BYTES = 160   # RenderParams per frame, passed by value to the launch
+METRIC = "Mrays/s and 4K frame ms, plain FP32 RK4 (3840x2160 Kerr-Newman a*=0.8 q=0.3 orbit)"
+CONFIG = {"workload": "kn_a0.8_q0.3_r25_incl75_fov45_3840x2160_orbit",
+          "frames_per_step": FRAMES_PER_STEP, "orbit_frames": ORBIT_FRAMES,
+          "step": "30 frames: every 10th frame of the 300-frame orbit (azimuth 360 k / 300 deg), offset by the rank",
+          "width": W, "height": H, "preset": "balanced dPhi=0.012 maxSteps=2000",
+          "scene": "disk + hot spots on (diskTime 0), bloom + tonemap on, exposure 1",
+          "precision": "fp32", "l2": "flushed (256 MiB memset) before every timed step; frame buffers > L2"}
 
 
 def parse():
@@ -89,12 +89,18 @@ def parse():
 
 
 def workload(derive, rank=0):
+    """The 30 orbit frames of a rank (distinct frames per rank, weak scaling)."""
     from bhrt import ranks, scenes
-    frames = scenes.kerr_pair_1080(derive, W, H, FRAMES_PER_SCENE)
-    times = ranks.frame_times_for_rank([P.diskTime for P in frames], rank)   # weak scaling: distinct frames
-    for P, t in zip(frames, times):
-        P.diskTime = t
-    return frames
+    ids = ranks.orbit_frames_for_rank(ORBIT_FRAMES, FRAMES_PER_STEP, rank)
+    return scenes.kn_orbit_4k(derive, W, H, ORBIT_FRAMES, ids)
+
+
+def _peaks():
+    try:
+        with open(os.path.join(ROOT, "MEASURED_PEAKS.json")) as fh:
+            return json.load(fh)
+    except (OSError, ValueError):
+        return {}
 
 
 # ---------------------------------------------------------------------------
@@ -164,7 +170,8 @@ class ClockSampler:
 
 
 # ---------------------------------------------------------------------------
-# CPU-baseline leg: the reference's tracer on the host cores + its work census
+# baseline legs: the reference's tracer on the host cores (+ the work census)
+# and the reference's own GPU kernel
 # ---------------------------------------------------------------------------
 def sample_pixels(frame_idx, stride, W_, H_):
     ys = np.arange((frame_idx * 7) % stride, H_, stride)
@@ -173,14 +180,11 @@ def sample_pixels(frame_idx, stride, W_, H_):
     return (yy * W_ + xx).ravel().astype(np.int32)
 
 
-def cpu_baseline_leg(frames, seconds):
-    """Time the reference tracer on a pixel sample of the workload, and count
-    the reference's algorithmic work (RK4 steps, disk sub-samples, escapes) on
-    the same frames for the FLOP accounting."""
+def work_census(frames):
+    """The reference's algorithmic work on the frames: the restated oracle
+    (bit-exact with the reference) on a 1/24^2 pixel sample of every frame."""
     sys.path.insert(0, os.path.join(ROOT, "oracle"))
     import oracle as orc
-    cores = os.cpu_count() or 1
-    # census: restated oracle (bit-exact with the reference) on a 1/24^2 sample of every frame
     port = orc.Oracle()
     census = []
     for k, P in enumerate(frames):
@@ -190,37 +194,80 @@ def cpu_baseline_leg(frames, seconds):
                  + rec["diskSamples"] * C_DISK + (rec["outcome"] == 1) * C_BG)
         census.append({"flops_per_ray": float(flops.mean()), "steps_per_ray": float(rec["steps"].mean()),
                        "disk_per_ray": float(rec["diskSamples"].mean())})
-    # timing: the reference's own build when present, else the restated port
+    return census
+
+
+def cpu_baseline_leg(frames, seconds):
+    """The reference tracer on a pixel sample of the workload, all host cores."""
+    sys.path.insert(0, os.path.join(ROOT, "oracle"))
+    import oracle as orc
+    cores = os.cpu_count() or 1
     kind = "reference" if orc.RefHost.available() else "port"
-    ref = orc.RefHost() if kind == "reference" else None
+    ref = orc.RefHost() if kind == "reference" else orc.Oracle()
     done, t0, chunks = 0, time.perf_counter(), 0
     while True:
         k = chunks % len(frames)
-        pix = sample_pixels(k + 31 * (chunks // len(frames)), 16, frames[k].width, frames[k].height)
-        if ref is not None:
+        pix = sample_pixels(k + 31 * (chunks // len(frames)), 64, frames[k].width, frames[k].height)
+        if kind == "reference":
             ref.render_pixels(frames[k], pix, threads=cores)
         else:
-            port.trace_pixels(frames[k], pix, threads=cores)
+            ref.trace_pixels(frames[k], pix, threads=cores)
         done += len(pix)
         chunks += 1
         if time.perf_counter() - t0 >= seconds and chunks >= len(frames):
             break
     el = time.perf_counter() - t0
     return {"value": done / el / 1e6, "unit": "Mrays/s", "cores": cores, "kind": kind,
-            "sample": f"{done} rays: 1/256 strided pixel samples of the 16 workload frames, "
-                      f"{el:.1f} s on {cores} threads"}, census
+            "sample": f"{done} rays: 1/64^2 strided pixel samples of the {len(frames)} workload frames, "
+                      f"{el:.1f} s on {cores} threads"}
+
+
+def reference_gpu_leg(frames, fs, flush, our_frame_ms):
+    """The reference's black_hole_kernel.cu, unchanged, built for sm_100a with its own flags
+    (oracle/_ref/libbhref_gpu.so): launchRenderPipeline on the same frames and buffers."""
+    import ctypes as C
+    import torch
+    sys.path.insert(0, os.path.join(ROOT, "oracle"))
+    import oracle as orc
+    if not orc.RefGpu.available():
+        return {"unavailable": "oracle/_ref/libbhref_gpu.so not built (reference tree absent at build time)"}
+    R = orc.RefGpu().lib
+    stream = torch.cuda.current_stream()
+    sp = C.c_void_p(stream.cuda_stream)
+    ptr = lambda t: C.c_void_p(t.data_ptr())  # noqa: E731
+
+    def run(evs=None):
+        for i, (P, f) in enumerate(zip(frames, fs)):
+            if evs is not None:
+                evs[i][0].record(stream)
+            code = R.launchRenderPipeline(ptr(f.out), ptr(f.accum), ptr(f.bloomA), ptr(f.bloomB), C.byref(P), sp)
+            if code != 0:
+                raise RuntimeError(f"reference launchRenderPipeline failed: {code}")
+            if evs is not None:
+                evs[i][1].record(stream)
+
+    run()
+    torch.cuda.synchronize()
+    flush.zero_()
+    evs = [[torch.cuda.Event(enable_timing=True) for _ in range(2)] for _ in frames]
+    run(evs)
+    torch.cuda.synchronize()
+    ms = np.array([a.elapsed_time(b) for a, b in evs])
+    med = float(np.median(ms))
+    return {"kernel": "reference src/black_hole_kernel.cu built unchanged for sm_100a (--use_fast_math, "
+                      "CMakeLists.txt:63)", "frame_ms": med, "mrays_s": W * H / (med * 1e-3) / 1e6,
+            "frames": len(frames), "speedup_of_this_build": med / our_frame_ms}
 
 
 # ---------------------------------------------------------------------------
 # our arm
 # ---------------------------------------------------------------------------
 def run_b200(args, rank, world, local_rank):
+    import ctypes as C
     import torch
     import torch.distributed as dist
-    from bhrt import lib
-    from bhrt.abi import BHView
+    from bhrt import lib, ranks
     from bhrt.device import Frame, measure_fp32_peak
-    import ctypes as C
 
     torch.cuda.set_device(local_rank)
     dev = torch.device("cuda", local_rank)
@@ -233,16 +280,8 @@ def run_b200(args, rank, world, local_rank):
     ptr = lambda t: C.c_void_p(t.data_ptr())  # noqa: E731
     flush = torch.empty(L2_FLUSH_BYTES, dtype=torch.uint8, device=dev)
     peak = measure_fp32_peak()
-    views = (BHView * nF)()
-    for i, (P, fr) in enumerate(zip(frames, fs)):
-        views[i].params = P
-        views[i].out, views[i].accum = fr.out.data_ptr(), fr.accum.data_ptr()
-        views[i].bloomA, views[i].bloomB = fr.bloomA.data_ptr(), fr.bloomB.data_ptr()
 
-    def batch():
-        lib.check(L.bhRenderBatch(views, nF, sp), "bhRenderBatch")
-
-    def per_frame(evs=None):
+    def step(evs=None):
         for i, (P, fr) in enumerate(zip(frames, fs)):
             if evs is not None:
                 evs[i][0].record(stream)
@@ -257,44 +296,33 @@ def run_b200(args, rank, world, local_rank):
     clocks = ClockSampler(local_rank)
     clocks.start()
     for _ in range(args.warmup):
-        batch()
-        per_frame()
+        step()
     torch.cuda.synchronize()
 
-    ev = [(torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)) for _ in range(args.steps)]
+    evs = [[[torch.cuda.Event(enable_timing=True) for _ in range(3)] for _ in range(nF)] for _ in range(args.steps)]
     if world > 1:
         dist.barrier()
     torch.cuda.synchronize()
     clocks.mark_start()
     for s in range(args.steps):
         flush.zero_()
-        ev[s][0].record(stream)
-        batch()
-        ev[s][1].record(stream)
+        step(evs[s])
     torch.cuda.synchronize()
     clocks.mark_stop()
     if world > 1:
         dist.barrier()
     clk = clocks.stop()
-    step_ms = np.array([a.elapsed_time(b) for a, b in ev])
-    total_ms = float(step_ms.sum())
-
-    # the per-frame form of the same job (bhRenderAccum + bhPostProcess per frame): trace / post split
-    evs = [[[torch.cuda.Event(enable_timing=True) for _ in range(3)] for _ in range(nF)] for _ in range(args.steps)]
-    for s in range(args.steps):
-        flush.zero_()
-        per_frame(evs[s])
-    torch.cuda.synchronize()
+    step_ms = np.array([evs[s][0][0].elapsed_time(evs[s][-1][2]) for s in range(args.steps)])
     trace_ms = np.array([[evs[s][i][0].elapsed_time(evs[s][i][1]) for i in range(nF)] for s in range(args.steps)])
     post_ms = np.array([[evs[s][i][1].elapsed_time(evs[s][i][2]) for i in range(nF)] for s in range(args.steps)])
-    pf_total = float((trace_ms + post_ms).sum())
-    # tracing time inside the batch: the step minus its 16 bloom + tonemap passes
-    batch_trace_total = total_ms - float(np.median(post_ms)) * nF * args.steps
+    total_ms = float(step_ms.sum())
+    trace_total = float(trace_ms.sum())
+    frame_ms = float(np.median(trace_ms + post_ms))
 
     # e2e: the reference-facing call per frame, params from the host, each RGBA8 frame read back to
     # pinned host memory on a copy stream (overlapping the next frame's tracing); the step ends when
     # the last read-back has landed
-    hosts = [torch.empty((H, W, 4), dtype=torch.uint8, pin_memory=True) for _ in range(nF)]
+    hosts = [torch.empty((H, W, 4), dtype=torch.uint8, pin_memory=True) for _ in range(2)]
     side = torch.cuda.Stream(device=dev)
     sps = (sp, C.c_void_p(side.cuda_stream))
     e2 = [(torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)) for _ in range(args.steps)]
@@ -304,50 +332,74 @@ def run_b200(args, rank, world, local_rank):
             e2[s][0].record(stream)
         side.wait_stream(stream)
         for i, (P, fr) in enumerate(zip(frames, fs)):
-            # frames alternate between two streams, so one frame's tail overlaps the next frame
             st = stream if i % 2 == 0 else side
             lib.check(L.launchRenderPipeline(ptr(fr.out), ptr(fr.accum), ptr(fr.bloomA), ptr(fr.bloomB),
                                              C.byref(P), sps[i % 2]), "launchRenderPipeline")
             with torch.cuda.stream(st):
-                hosts[i].copy_(fr.out, non_blocking=True)
+                hosts[i % 2].copy_(fr.out, non_blocking=True)
         stream.wait_stream(side)
         if s >= 0:
             e2[s][1].record(stream)
     torch.cuda.synchronize()
     e2e_ms = float(sum(a.elapsed_time(b) for a, b in e2))
 
-    from bhrt import ranks
-    total_ms, e2e_ms, trace_total, pf_total = ranks.max_over_ranks(
-        [total_ms, e2e_ms, batch_trace_total, pf_total], world, dev)
+    total_ms, e2e_ms, trace_total = ranks.max_over_ranks([total_ms, e2e_ms, trace_total], world, dev)
     rays_step = nF * W * H
     out = {
-        "metric": "Mrays/s (plain FP32 RK4, 1920x1080 Kerr/Kerr-Newman pair, 16 frames)",
+        "metric": METRIC,
         "value": world * rays_step * args.steps / (total_ms * 1e-3) / 1e6,
         "unit": "Mrays/s",
         "n_gpus": world, "steps": args.steps, "warmup": args.warmup,
         "ms_per_step": total_ms / args.steps,
-        "frame_ms": total_ms / args.steps / nF,
-        "api": "bhRenderBatch: the 16 frames of a step traced from one work queue (one persistent launch), "
-               "then 16 bloom + tonemap passes",
-        "per_frame_path": {"value": world * rays_step * args.steps / (pf_total * 1e-3) / 1e6, "unit": "Mrays/s",
-                           "api": "bhRenderAccum + bhPostProcess per frame",
-                           "frame_ms": float(np.median(trace_ms + post_ms)),
-                           "trace_ms_per_frame": float(np.median(trace_ms)),
-                           "post_ms_per_frame": float(np.median(post_ms))},
+        "frame_ms": frame_ms,
+        "trace_ms_per_frame": float(np.median(trace_ms)),
+        "post_ms_per_frame": float(np.median(post_ms)),
+        "api": "bhRenderAccum + bhPostProcess per frame (= launchRenderPipeline), device-resident",
         "higher_is_better": True, "scaling": "weak", "vs_baseline": None,
-        "dtype": "f32", "data": "synthetic (procedural scenes of the named configuration)",
-        "config": {"workload": "kerr_a0.9+kn_a-0.7_q0.4_1920x1080_8frames_each_bloom",
-                   "frames_per_step": nF, "width": W, "height": H, "preset": "balanced dPhi=0.012 maxSteps=2000",
-                   "camera": "r=20 rs, inclination 80 deg, FOV 45 deg", "precision": "fp32",
-                   "l2": "flushed (256 MiB memset) before every timed step",
-                   "parallelism": f"replicas x{world} (frames per rank, no collective)"},
+        "dtype": "f32", "data": "synthetic (procedural scene of the named configuration)",
+        "config": dict(CONFIG, parallelism=f"replicas x{world} (frames per rank, no collective)"),
         "e2e": {"value": world * rays_step * args.steps / (e2e_ms * 1e-3) / 1e6, "unit": "Mrays/s",
-                "h2d_bytes_per_step": nF * RAY_BYTES, "d2h_bytes_per_step": nF * W * H * 4},
-        "gpu_launches": args.steps * (1 + nF * 2),
+                "api": "launchRenderPipeline per frame + RGBA8 read-back to pinned host memory",
+                "h2d_bytes_per_step": nF * PARAM_BYTES, "d2h_bytes_per_step": nF * W * H * 4},
+        "gpu_launches": args.steps * nF * 3,
         "clocks": clk,
         "fp32_peak_tflops_measured": peak,
     }
-    return out, trace_total
+    return out, trace_total, frames, fs, flush
+
+
+def kerr_pair_leg(steps=3):
+    """The 1920x1080 Kerr a*=+0.9 / Kerr-Newman a*=-0.7 q=0.4 pair (r = 20, inclination 80, FOV 45,
+    8 frames each, disk + hot spots + bloom): the 16 frames through one bhRenderBatch, L2 flushed."""
+    import ctypes as C
+    import torch
+    from bhrt import lib, scenes
+    from bhrt.abi import BHView
+    from bhrt.device import Frame
+    L = lib.load()
+    frames = scenes.kerr_pair_1080(lib.derive, 1920, 1080, 8)
+    fs = [Frame(1920, 1080) for _ in frames]
+    views = (BHView * len(frames))()
+    for i, (P, fr) in enumerate(zip(frames, fs)):
+        views[i].params = P
+        views[i].out, views[i].accum = fr.out.data_ptr(), fr.accum.data_ptr()
+        views[i].bloomA, views[i].bloomB = fr.bloomA.data_ptr(), fr.bloomB.data_ptr()
+    sp = C.c_void_p(torch.cuda.current_stream().cuda_stream)
+    flush = torch.empty(L2_FLUSH_BYTES, dtype=torch.uint8, device="cuda")
+    e0, e1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+    lib.check(L.bhRenderBatch(views, len(frames), sp), "bhRenderBatch")
+    ts = []
+    for _ in range(steps):
+        flush.zero_()
+        e0.record()
+        lib.check(L.bhRenderBatch(views, len(frames), sp), "bhRenderBatch")
+        e1.record()
+        torch.cuda.synchronize()
+        ts.append(e0.elapsed_time(e1))
+    ms = float(np.median(ts))
+    return {"workload": "kerr_a0.9+kn_a-0.7_q0.4_1920x1080_8frames_each_bloom (16 frames per call)",
+            "api": "bhRenderBatch", "ms_per_16_frames": ms, "frame_ms": ms / len(frames),
+            "mrays_s": len(frames) * 1920 * 1080 / (ms * 1e-3) / 1e6}
 
 
 # ---------------------------------------------------------------------------
@@ -394,11 +446,7 @@ def surrogate_leg():
         mlp_ms = e0.elapsed_time(e1) / 5
         del x, y
         flops = 2.0 * (4 * 256 * 256 + 256 * 16) * n
-        peaks = {}
-        try:
-            peaks = json.load(open(os.path.join(ROOT, "MEASURED_PEAKS.json")))
-        except OSError:
-            pass
+        peaks = _peaks()
         bf16_peak = peaks.get("bf16_tflops", 1590.0)
         fa, fb = Frame(SG_W, SG_H), Frame(SG_W, SG_H)
 
@@ -468,7 +516,7 @@ def surrogate_leg():
 
 
 # ---------------------------------------------------------------------------
-# configuration legs (single GPU): mixed precision at 4K, the 256-view batch
+# configuration legs (single GPU)
 # ---------------------------------------------------------------------------
 def mixed_leg():
     """3840x2160 Kerr-Newman a*=0.998 (0.995 after the clamp) q=0.05, r=12, FOV 50, elevation sweep:
@@ -589,12 +637,7 @@ def post_leg():
     f.pipeline(P)
     flush = torch.empty(L2_FLUSH_BYTES, dtype=torch.uint8, device="cuda")
     e0, e1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
-    peaks = {}
-    try:
-        with open(os.path.join(ROOT, "MEASURED_PEAKS.json")) as fh:
-            peaks = json.load(fh)
-    except (OSError, ValueError):
-        pass
+    peaks = _peaks()
     hbm = peaks.get("hbm_gbs", 6650.0)
     res = {"workload": "bhPostProcess on kn_a0.998_q0.05_r12_fov50_3840x2160 frame 60 (accum 133 MB > L2, "
                        "L2 flushed per launch)",
@@ -671,6 +714,35 @@ def batch256_leg():
             "sequential_mrays_s": mr(t_seq), "batch_mrays_s": mr(t_batch), "graph_mrays_s": mr(t_graph)}
 
 
+def highlights(out):
+    """The figures of every leg in one short object, last on the line."""
+    h = {"frame_ms": out.get("frame_ms"), "value_mrays_s": out.get("value"),
+         "e2e_mrays_s": out.get("e2e", {}).get("value"), "roofline_frac": out.get("roofline", {}).get("frac")}
+    rg = out.get("reference_gpu_kernel", {})
+    if "frame_ms" in rg:
+        h["reference_gpu_frame_ms"] = rg["frame_ms"]
+        h["speedup_over_reference_gpu"] = rg["speedup_of_this_build"]
+    sg = out.get("surrogate")
+    if sg:
+        for g, r in sg["gates"].items():
+            h[f"surrogate_{g}"] = {"frame_ms": r["frame_ms"], "speedup": r["speedup_vs_plain"],
+                                   "px_within_1lsb": r["px_within_1lsb"], "rk4_frac": r["rk4_pixel_frac"]}
+        h["surrogate_mlp_frac"] = sg["mlp"]["roofline"]["frac"]
+    mx = out.get("mixed_precision_4k")
+    if mx:
+        acc89 = mx["accuracy_vs_fp64_by_elevation_deg"].get("89.0", {})
+        h["mixed_vs_fp32_time"] = mx["mixed_over_fp32_time"]
+        h["esc_1e4_at_89deg"] = {k: v["escape_dir_err_rad"]["frac_within_1e-4"] for k, v in acc89.items()}
+    if out.get("batch_256_views"):
+        b = out["batch_256_views"]
+        h["batch256_ms"] = {"sequential": b["sequential_ms"], "batch": b["batch_ms"], "graph": b["graph_ms"]}
+    if out.get("post_process"):
+        h["post_frac_bloom_on"] = out["post_process"]["bloom_on"]["frac"]
+    if out.get("kerr_pair_1080"):
+        h["kerr_pair_1080_mrays_s"] = out["kerr_pair_1080"]["mrays_s"]
+    return h
+
+
 def main():
     args = parse()
     rank = int(os.environ.get("RANK", "0"))
@@ -682,35 +754,41 @@ def main():
             return
         return run_reference(args)
 
-    import torch
     import torch.distributed as dist
     if world > 1:
         from datetime import timedelta
         dist.init_process_group("nccl", timeout=timedelta(seconds=120))
-    out, trace_total_ms = run_b200(args, rank, world, local_rank)
+    out, trace_total_ms, frames, fs, flush = run_b200(args, rank, world, local_rank)
     if rank == 0:
-        from bhrt import lib
-        frames = workload(lib.derive, 0)
         if not args.no_cpu_baseline:
-            base, census = cpu_baseline_leg(frames, args.baseline_seconds)
-            flops_frame = [c["flops_per_ray"] * W * H for c in census]
-            flops_step = float(sum(flops_frame))
+            census = work_census(frames)
+            flops_step = float(sum(c["flops_per_ray"] * W * H for c in census))
             achieved = flops_step * args.steps / (trace_total_ms * 1e-3) / 1e12
             peak = out["fp32_peak_tflops_measured"]
             out["roofline"] = {"bound": "fp32", "achieved": achieved, "peak": peak, "unit": "TFLOP/s",
                                "frac": achieved / peak if peak else None, "traffic": None,
-                               "peak_source": "measured FP32 FMA microbenchmark, max of scalar and packed fma.rn.f32x2 "
-                                              "(bhMeasureFp32Peak), same run",
+                               "peak_source": "measured FP32 FMA microbenchmark, max of scalar and packed "
+                                              "fma.rn.f32x2 (bhMeasureFp32Peak), same run",
+                               "kernel": "tile_kernel<KerrRay<float>> (bhRenderAccum)",
                                "flops_per_frame": flops_step / len(frames),
                                "steps_per_ray": float(np.mean([c["steps_per_ray"] for c in census]))}
-            out["cpu_baseline"] = base
+            out["cpu_baseline"] = cpu_baseline_leg(frames, args.baseline_seconds)
+            if world == 1:
+                out["reference_gpu_kernel"] = reference_gpu_leg(frames, fs, flush, out["frame_ms"])
+        del fs, flush
         if world == 1 and not args.no_configs:
+            import torch
+            torch.cuda.empty_cache()
+            out["kerr_pair_1080"] = kerr_pair_leg()
             out["mixed_precision_4k"] = mixed_leg()
             out["batch_256_views"] = batch256_leg()
             out["post_process"] = post_leg()
             out["accuracy"] = accuracy_leg()
         if world == 1 and not args.no_surrogate:
+            import torch
+            torch.cuda.empty_cache()
             out["surrogate"] = surrogate_leg()
+        out["highlights"] = highlights(out)
         print(json.dumps(out))
     if world > 1:
         dist.barrier()
@@ -718,13 +796,19 @@ def main():
 
 
 def run_reference(args):
+    """The reference's own tracer (src/trace.cuh and post_process.cuh built as host
+    code, oracle/_ref) on the host cores, on the same frames as this build's arm.
+    Scenes are derived with the reference's own bhValidateAndDerive, so nothing of
+    this build is loaded; each step traces a 1/6^2 strided pixel sample of one
+    workload frame through the reference's renderSampleHDR."""
     sys.path.insert(0, os.path.join(ROOT, "oracle"))
     import oracle as orc
-    from bhrt import lib
-    frames = workload(lib.derive, 0)
     cores = os.cpu_count() or 1
-    kind = "reference" if orc.RefHost.available() else "port"
-    impl = orc.RefHost() if kind == "reference" else orc.Oracle()
+    if orc.RefHost.available():
+        kind, impl = "reference", orc.RefHost()
+    else:
+        kind, impl = "port", orc.Oracle()
+    frames = workload(impl.derive, 0)
 
     def one(k):
         P = frames[k % len(frames)]
@@ -741,15 +825,15 @@ def run_reference(args):
     n = sum(one(args.warmup + k) for k in range(args.steps))
     el = time.perf_counter() - t0
     v = n / el / 1e6
-    out = {"impl": "reference",
-           "metric": "Mrays/s (plain FP32 RK4, 1920x1080 Kerr/Kerr-Newman pair, 16 frames)",
+    out = {"impl": "reference", "metric": METRIC,
            "value": v, "unit": "Mrays/s", "n_gpus": 1, "steps": args.steps, "warmup": args.warmup,
-           "ms_per_step": el * 1e3 / args.steps, "higher_is_better": True, "scaling": "weak",
-           "vs_baseline": None, "dtype": "f32", "data": "synthetic",
-           "config": {"workload": "kerr_a0.9+kn_a-0.7_q0.4_1920x1080_8frames_each_bloom",
-                      "sample": "each step traces a 1/6^2 strided pixel sample of one workload frame"},
+           "ms_per_step": el * 1e3 / args.steps, "frame_ms": W * H / (v * 1e6) * 1e3,
+           "higher_is_better": True, "scaling": "weak",
+           "vs_baseline": None, "dtype": "f32", "data": "synthetic (procedural scene of the named configuration)",
+           "config": dict(CONFIG, parallelism="replicas x1 (frames per rank, no collective)"),
            "cpu_baseline": {"value": v, "unit": "Mrays/s", "cores": cores, "kind": kind,
-                            "sample": f"{n} rays over {args.steps} steps on {cores} threads"},
+                            "sample": f"{n} rays over {args.steps} steps (1/6^2 strided pixel samples of the "
+                                      f"workload frames) on {cores} threads"},
            "e2e": {"value": v, "unit": "Mrays/s", "h2d_bytes_per_step": 0, "d2h_bytes_per_step": 0}}
     print(json.dumps(out))
 

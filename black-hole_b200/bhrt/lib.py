@@ -44,6 +44,7 @@ _SIGNATURES = {
     "bhAutotuneBatch": (_int, [_vp, _int, C.POINTER(_int), C.POINTER(_int), C.POINTER(C.c_float)]),
     "bhRenderPipelineNoAlloc": (_int, [_vp, _vp, _P, _vp]),
     "bhMeasureFp32Peak": (C.c_double, []),
+    "bhLibraryDeviceBytes": (C.c_ulonglong, [_int]),
     "bhTcGemm": (_int, [_vp, _int, _vp, _int, _vp, _int, _int, _int, _int, _int, _int, _vp, _vp]),
     "bhTcErrorFlags": (_int, [C.POINTER(C.c_uint)]),
     "bhSurrogateParamCount": (_int, []),

@@ -15,6 +15,16 @@ def shard_views(views, rank, world):
     return list(views[rank::world])
 
 
+def orbit_frames_for_rank(n_orbit, per_rank, rank):
+    """Frame indices of a rank's replica of an orbit workload: `per_rank` frames
+    evenly spaced over the `n_orbit`-frame orbit, offset by the rank, so up to
+    n_orbit / per_rank ranks render distinct frames of equal cost on average."""
+    if per_rank < 1 or n_orbit < per_rank or rank < 0:
+        raise ValueError("bad orbit sharding")
+    stride = n_orbit // per_rank
+    return [(j * stride + rank) % n_orbit for j in range(per_rank)]
+
+
 def frame_times_for_rank(times, rank):
     """Animation times of a rank's replica: the workload's frame times shifted
     by the rank, so replicas render distinct frames of the same workload."""

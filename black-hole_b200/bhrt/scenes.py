@@ -165,6 +165,15 @@ def kn_sweep_4k(derive, width=3840, height=2160, frames=120, frame_ids=None):
     return out
 
 
+def kn_orbit_4k(derive, width=3840, height=2160, frames=300, frame_ids=None):
+    """Kerr-Newman a* = 0.8 q = 0.3 at r = 25, inclination 75 deg (elevation 15),
+    FOV 45, disk + hot spots, bloom + tonemap, static disk (diskTime 0): frame k
+    of the `frames`-frame orbit has camera azimuth 360 k / frames deg."""
+    ids = range(frames) if frame_ids is None else frame_ids
+    return [scene(derive, BH_KERR_NEWMAN, 0.8, 0.3, width, height, 25.0, 15.0, 45.0,
+                  az_deg=360.0 * k / frames) for k in ids]
+
+
 BATCH_RESOLUTIONS = ((128, 72), (320, 180), (640, 360), (1280, 720), (1920, 1080))
 
 

@@ -18,9 +18,24 @@
 #include "bh_internal.h"
 
 namespace {
+constexpr int kMaxDevices = 64;
+std::atomic<unsigned long long> gAllocBytes[kMaxDevices];
+}  // namespace
+
+// Every device allocation the library makes (caches, tables, workspaces of
+// handles) goes through here, so bhLibraryDeviceBytes can account for it.
+cudaError_t bh_device_alloc(void** p, size_t bytes)
+{
+    cudaError_t e = cudaMalloc(p, bytes);
+    int dev = 0;
+    if (e == cudaSuccess && cudaGetDevice(&dev) == cudaSuccess && dev >= 0 && dev < kMaxDevices)
+        gAllocBytes[dev].fetch_add(bytes);
+    return e;
+}
+
+namespace {
 
 // ---- per-device scratch: the ray counter of the work queue --------------------
-constexpr int kMaxDevices = 64;
 constexpr size_t kScratchBytes = 4096;
 std::mutex gScratchLock;
 unsigned* gScratch[kMaxDevices] = {};
@@ -54,7 +69,7 @@ cudaError_t deviceScratch(unsigned** out)
     if (!gScratch[dev])
     {
         void* p = nullptr;
-        e = cudaMalloc(&p, kScratchBytes);
+        e = bh_device_alloc(&p, kScratchBytes);
         if (e != cudaSuccess) return e;
         gScratch[dev] = static_cast<unsigned*>(p);
     }
@@ -107,7 +122,7 @@ cudaError_t tileOrder(int W, int H, const unsigned** out)
             c.dev = nullptr;
             c.cap = 0;
             void* p = nullptr;
-            e = cudaMalloc(&p, n * sizeof(unsigned));
+            e = bh_device_alloc(&p, n * sizeof(unsigned));
             if (e != cudaSuccess) return e;
             c.dev = static_cast<unsigned*>(p);
             c.cap = n;
@@ -230,7 +245,7 @@ cudaError_t pipeline(uchar4* out, float4* accum, float4* bloomA, float4* bloomB,
     if (!out || !accum || (P.bloomEnabled && (!bloomA || !bloomB))) return cudaErrorInvalidValue;
     cudaError_t e = trace(frameParams(P, BH_OUT_ACCUM, accum), P, precision, false, stream);
     if (e != cudaSuccess) return e;
-    return bh_launch_post(out, accum, bloomB, P.width, P.height, postConsts(P), stream);
+    return bh_launch_post(out, accum, bloomB, bloomA, P.width, P.height, postConsts(P), stream);
 }
 
 }  // namespace
@@ -285,11 +300,10 @@ cudaError_t bhRenderHDR(float4* hdr, const RenderParams& p, int precision, cudaS
 cudaError_t bhPostProcess(uchar4* out, const float4* accum, float4* bloomA, float4* bloomB,
                           const RenderParams& p, cudaStream_t stream)
 {
-    (void)bloomA;
     RenderParams P = p;
     bhSanitizeRenderParams(&P);
     if (!out || !accum || (P.bloomEnabled && !bloomB)) return cudaErrorInvalidValue;
-    return bh_launch_post(out, accum, bloomB, P.width, P.height, postConsts(P), stream);
+    return bh_launch_post(out, accum, bloomB, bloomA, P.width, P.height, postConsts(P), stream);
 }
 
 cudaError_t bhProbeGrid(BHProbe* out, const RenderParams& p, int nx, int ny, int precision,
@@ -340,6 +354,11 @@ void bhGetTuning(int family, int* refillMin, int* blocksPerSm)
 }
 
 double bhMeasureFp32Peak(void) { return bh_measure_fp32_peak(); }
+
+unsigned long long bhLibraryDeviceBytes(int device)
+{
+    return (device >= 0 && device < kMaxDevices) ? gAllocBytes[device].load() : 0ull;
+}
 
 const char* bhVersion(void) { return "libbh 0.1 (sm_100a)"; }
 

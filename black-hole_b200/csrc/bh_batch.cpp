@@ -100,7 +100,7 @@ cudaError_t launchPlan(const Plan& pl, const BHView* views, const TraceParams* d
     {
         const RenderParams& P = pl.params[i];
         PostConsts pc{P.exposure, P.bloomStrength, P.bloomEnabled ? 1 : 0, P.swapRB};
-        e = bh_launch_post(views[i].out, views[i].accum, views[i].bloomB, P.width, P.height, pc, s);
+        e = bh_launch_post(views[i].out, views[i].accum, views[i].bloomB, views[i].bloomA, P.width, P.height, pc, s);
         if (e != cudaSuccess) return e;
     }
     return cudaSuccess;
@@ -132,8 +132,8 @@ cudaError_t ensureTables(int n, DevTables** out)
         t.base = nullptr;
         t.cap = 0;
         size_t cap = std::max<size_t>(64, (size_t)n);
-        if ((e = cudaMalloc(&t.table, cap * sizeof(TraceParams))) != cudaSuccess) return e;
-        if ((e = cudaMalloc(&t.base, (cap + 2) * sizeof(unsigned))) != cudaSuccess) return e;
+        if ((e = bh_device_alloc(reinterpret_cast<void**>(&t.table), cap * sizeof(TraceParams))) != cudaSuccess) return e;
+        if ((e = bh_device_alloc(reinterpret_cast<void**>(&t.base), (cap + 2) * sizeof(unsigned))) != cudaSuccess) return e;
         t.cap = cap;
     }
     *out = &t;
@@ -218,9 +218,9 @@ extern "C" cudaError_t bhBatchGraphCreate(BHBatchGraph** out, const BHView* view
     cudaStream_t s = nullptr;
     const size_t tb = n * sizeof(TraceParams), bb = (n + 2) * sizeof(unsigned);
     if (e == cudaSuccess) e = cudaGetDevice(&G->device);
-    if (e == cudaSuccess) e = cudaMalloc(&G->dTable, tb);
-    if (e == cudaSuccess) e = cudaMalloc(&G->dBase, bb);
-    if (e == cudaSuccess) e = cudaMalloc(&G->dCounter, 256);
+    if (e == cudaSuccess) e = bh_device_alloc(reinterpret_cast<void**>(&G->dTable), tb);
+    if (e == cudaSuccess) e = bh_device_alloc(reinterpret_cast<void**>(&G->dBase), bb);
+    if (e == cudaSuccess) e = bh_device_alloc(reinterpret_cast<void**>(&G->dCounter), 256);
     if (e == cudaSuccess) e = cudaMallocHost(&G->hPinned, tb + bb);
     if (e == cudaSuccess) e = cudaEventCreateWithFlags(&G->done, cudaEventDisableTiming);
     if (e == cudaSuccess) e = cudaStreamCreateWithFlags(&s, cudaStreamNonBlocking);
@@ -296,7 +296,7 @@ extern "C" cudaError_t bhAutotune(const RenderParams& p, int* refillMin, int* bl
     cudaError_t e = bh_trace_max_blocks(P.model, &maxBlocks);
     if (e != cudaSuccess) return e;
     float4* hdr = nullptr;
-    if ((e = cudaMalloc(&hdr, (size_t)P.width * P.height * sizeof(float4))) != cudaSuccess) return e;
+    if ((e = bh_device_alloc(reinterpret_cast<void**>(&hdr), (size_t)P.width * P.height * sizeof(float4))) != cudaSuccess) return e;
     cudaStream_t s = nullptr;
     cudaEvent_t e0 = nullptr, e1 = nullptr;
     cudaStreamCreateWithFlags(&s, cudaStreamNonBlocking);

@@ -554,9 +554,21 @@ static __device__ __noinline__ KerrStep64 kerr_rk4_fp64(const CamFrame<double>& 
 // MIXED: FP32 state and steps; FP64 initial data (tetrad map and camera
 // position), whole steps in FP64 at radial turning points (p_r would change
 // sign within the step -- for near-extremal holes this includes periapses a
-// few percent outside the horizon), and FP64 bisection of the equatorial
+// few percent outside the horizon), FP64 state and steps through every polar
+// passage (|sin th| < 1/16, below), and FP64 bisection of the equatorial
 // crossing.  (FP64 steps over the whole final horizon approach were measured
 // to cost 70 % more time for no accuracy gain, and are not taken.)
+//
+// Polar passages.  A ray that passes within a small angle th_min of the spin
+// axis swings its azimuth by ~pi and reverses p_th within a few steps, and the
+// step's outcome depends on th relative to th_min: a rounding error e in an
+// FP32 state th becomes a relative error e / th_min of the passage (at
+// th_min ~ 3e-4, an FP32 rounding of ~1e-9 changes p_th after the passage by
+// ~1e-3 relative, and the escape direction by ~1e-4 rad).  FP64 arithmetic
+// inside each step does not help while the state is rounded back to FP32
+// between steps; what does is to carry an FP64 state from the step that enters
+// the cap |sin th| < 1/16 to the step that leaves it, so that is what MIXED
+// does (polar_passage_fp64).
 template <class R, bool STATS, bool MIXED = false>
 struct KerrRay
 {
@@ -678,6 +690,7 @@ struct KerrRay
         R dl0 = R(0), dl1 = R(0), dl2 = R(0);                 // the final stage's derivative
         if constexpr (MIXED)
         {
+            if (abs_p(s) < R(0.0625f)) return polar_passage_fp64(P);
             if (abs_p(pr) < h * abs_p(d1.pr))
             {
                 KerrStep64 o = kerr_rk4_fp64(P.cd, k.E, k.Lz, r, th, ph, pr, pth, h);
@@ -691,6 +704,8 @@ struct KerrRay
         kerr_rk4(F, k, h, r, th, ph, pr, pth, d1, d4);
         return finish_step(P, F, h, rS, thS, drS, dthS, d4.r, d4.th, d4.ph);
     }
+
+    BH_DEV bool polar_passage_fp64(const TraceParams& P);
 
     // Rest of a loop iteration after the RK4 update: pole guard, the next
     // step's first right-hand side with the slow-light term, disk chord.
@@ -791,3 +806,60 @@ struct KerrRay
                               (float)(-sth * sph * vr - cth * sph * vt - cph * vp)));
     }
 };
+
+// MIXED polar passage: the ray continues as an FP64 ray (same method, same
+// termination tests and disk chords, E and Lz as the FP32 ray holds them) with
+// its state carried in FP64 from step to step, until it leaves the cap
+// |sin th| < 1/16 or terminates; then the state is rounded back once.  The
+// step that decided to enter is taken here, so the call advances at least one
+// step.  Returns true when the ray terminated.  Out of line: the FP32 step
+// loop keeps its register budget.
+template <class R, bool STATS, bool MIXED>
+__device__ __noinline__ bool KerrRay<R, STATS, MIXED>::polar_passage_fp64(const TraceParams& P)
+{
+    if constexpr (MIXED && std::is_same<R, float>::value)
+    {
+        const CamFrame<double>& D = P.cd;
+        KerrRay<double, STATS, false> d;
+        const double E = k.E, Lz = k.Lz;
+        d.k = KerrConsts<double>{E, Lz, D.a * E, E * D.a2 - D.a * Lz, 4.0 * E};
+        d.r = r; d.th = th; d.ph = ph; d.pr = pr; d.pth = pth;
+        sincos_theta(d.th, d.s, d.c);
+        KerrEval<double> ev = kerr_rhs(D, d.k, d.r, d.s, d.c, d.pr, d.pth);
+        d.d1 = ev.d;
+        d.K1 = ev.K;
+        d.tFlight = tFlight;
+        d.prevPos = prevPos; d.accum = accum; d.trans = trans; d.maxHviol = maxHviol;
+        d.step = step; d.horizon = horizon; d.escaped = escaped; d.useDeriv = useDeriv;
+        if (STATS) { d.tally = tally; d.Q0 = Q0; }
+        bool done = false;
+        // bounded by the step budget: every iteration takes a step or terminates
+        while (!(done = d.advance(P)))
+            if (abs_p(d.s) >= 0.0625) break;
+        r = (R)d.r; th = (R)d.th; ph = (R)d.ph; pr = (R)d.pr; pth = (R)d.pth;
+        tFlight = (R)d.tFlight;
+        prevPos = d.prevPos; accum = d.accum; trans = d.trans; maxHviol = d.maxHviol;
+        step = d.step; horizon = d.horizon; escaped = d.escaped; useDeriv = d.useDeriv;
+        if (STATS) tally = d.tally;
+        if (done && escaped && useDeriv && step >= P.maxSteps)
+        {   // budget exhausted inside the passage: the last stage's derivative
+            const double* dd = KerrRay<double, STATS, false>::last_deriv();
+            R* dl = last_deriv();
+            dl[0] = (R)dd[0]; dl[1] = (R)dd[1]; dl[2] = (R)dd[2];
+        }
+        if (done)
+        {   // pack() reads the escape derivative from d1
+            d1.r = (R)d.d1.r; d1.th = (R)d.d1.th; d1.ph = (R)d.d1.ph; d1.pr = (R)d.d1.pr; d1.pth = (R)d.d1.pth;
+            K1 = (R)d.K1;
+            sincos_theta(th, s, c);
+            return true;
+        }
+        // back to FP32: the next step's first right-hand side from the rounded state
+        sincos_theta(th, s, c);
+        KerrEval<R> e32 = kerr_rhs(frame_of<R>(P), k, r, s, c, pr, pth);
+        d1 = e32.d;
+        K1 = e32.K;
+        return false;
+    }
+    return false;
+}

@@ -34,9 +34,13 @@ cudaError_t bh_launch_batch(bool kerr, const TraceParams* views, const unsigned*
 // resident CTAs per SM of the FP32 tracing kernel of a model's family
 cudaError_t bh_trace_max_blocks(int model, int* out);
 
-// bloom + tonemap of an accumulation buffer (bh_post.cu); `hblur` holds the
-// horizontally blurred half-resolution image ((W+1)/2 x (H+1)/2 float4)
-cudaError_t bh_launch_post(uchar4* out, const float4* accum, float4* hblur, int W, int H,
+// cudaMalloc, counted per device for bhLibraryDeviceBytes (bh_api.cpp)
+cudaError_t bh_device_alloc(void** p, size_t bytes);
+
+// bloom + tonemap of an accumulation buffer (bh_post.cu); `hblur` receives the
+// horizontally blurred half-resolution image ((W+1)/2 x (H+1)/2 float4) and,
+// when not null, `vblur` the finished (vertically blurred) bloom of the same size
+cudaError_t bh_launch_post(uchar4* out, const float4* accum, float4* hblur, float4* vblur, int W, int H,
                            const PostConsts& pc, cudaStream_t stream);
 
 // frame constants of a sanitised view for the given output (bh_api.cpp), and

@@ -4,11 +4,10 @@
 // launchRenderPipeline needs two pieces of scratch memory besides the caller's
 // buffers: the work counter the persistent tracing kernel draws rays from, and
 // a tile-order table, both allocated by the library on first use.  Some
-// callers cannot let a library allocate: a render loop that runs inside CUDA
-// stream capture (cudaMalloc is not allowed while a capture is open), a
-// real-time frame loop that must never stall on the allocator (an allocation
-// can synchronise the device), or a plugin whose host framework owns every
-// byte of device memory and hands out only the buffers it manages.  For them
+// callers cannot let a library allocate: a plugin whose host framework owns
+// every byte of device memory and hands out only the buffers it manages, or a
+// real-time frame loop that must never stall on the allocator (cudaMalloc can
+// synchronise the device).  For them
 // this file holds all the scratch in one file-scope __device__ array of fixed
 // size, loaded with the module; the entry point below allocates nothing.
 //
@@ -20,10 +19,12 @@
 //   * every call on a device uses the same array, which keeps the previous
 //     call's contents (the counter is cleared on the stream before each
 //     trace), so calls that overlap on the GPU race: serialise them;
+//   * the array belongs to this library's module: under lazy module loading
+//     (the CUDA default) the module, and with it the array, is loaded on a
+//     device at the first call there; later calls allocate nothing;
 //   * tiles are traced in row-major order (no order table); the image is the
 //     same as launchRenderPipeline's.
 // ---------------------------------------------------------------------------
-#include <mutex>
 #include <cuda_runtime.h>
 #include "bh_launch.h"
 #include "bh_internal.h"
@@ -36,28 +37,17 @@ constexpr size_t kScratchBytes = kHeaderBytes + (size_t)BH_NOALLOC_MAX_HALF_PIXE
 // Every GPU that loads libbh.so holds this array until the process exits.
 static __device__ __align__(256) unsigned char gNoAllocScratch[kScratchBytes];
 
-constexpr int kMaxDevices = 64;
-std::mutex gLock;
-unsigned char* gAddr[kMaxDevices] = {};
-
-// Device address of the array on the current device (host code cannot use
-// the symbol itself: on the host it names a stand-in, not device memory).
-// Looked up once per device, on that device's first call.
+// Device address of the array in the current device's context (host code
+// cannot use the symbol itself: on the host it names a stand-in, not device
+// memory).  Looked up on every call, so a device reset or another context
+// never leaves a stale address; the lookup allocates nothing once the module
+// is loaded.
 cudaError_t scratch_address(unsigned char** out)
 {
-    int dev = 0;
-    cudaError_t e = cudaGetDevice(&dev);
+    void* p = nullptr;
+    cudaError_t e = cudaGetSymbolAddress(&p, gNoAllocScratch);
     if (e != cudaSuccess) return e;
-    if (dev < 0 || dev >= kMaxDevices) return cudaErrorInvalidDevice;
-    std::lock_guard<std::mutex> g(gLock);
-    if (!gAddr[dev])
-    {
-        void* p = nullptr;
-        e = cudaGetSymbolAddress(&p, gNoAllocScratch);
-        if (e != cudaSuccess) return e;
-        gAddr[dev] = static_cast<unsigned char*>(p);
-    }
-    *out = gAddr[dev];
+    *out = static_cast<unsigned char*>(p);
     return cudaSuccess;
 }
 
@@ -82,6 +72,6 @@ extern "C" cudaError_t bhRenderPipelineNoAlloc(uchar4* out, float4* accum, const
     e = bh_launch_trace(t, BH_PREC_FP32, false, bh_family_blocks(P), stream);
     if (e != cudaSuccess) return e;
     PostConsts pc{P.exposure, P.bloomStrength, P.bloomEnabled ? 1 : 0, P.swapRB};
-    return bh_launch_post(out, accum, reinterpret_cast<float4*>(base + kHeaderBytes), P.width, P.height, pc,
+    return bh_launch_post(out, accum, reinterpret_cast<float4*>(base + kHeaderBytes), nullptr, P.width, P.height, pc,
                           stream);
 }

@@ -86,7 +86,7 @@ double bh_measure_fp32_peak()
     if (cudaDeviceGetAttribute(&sms, cudaDevAttrMultiProcessorCount, dev) != cudaSuccess) return 0.0;
     float* out = nullptr;
     const int blocks = sms * 8;
-    if (cudaMalloc(&out, blocks * sizeof(float)) != cudaSuccess) return 0.0;
+    if (bh_device_alloc(reinterpret_cast<void**>(&out), blocks * sizeof(float)) != cudaSuccess) return 0.0;
     const float best = fminf(best_ms(fma_kernel, out, blocks), best_ms(fma2_kernel, out, blocks));
     cudaFree(out);
     if (cudaGetLastError() != cudaSuccess) return 0.0;

@@ -9,12 +9,14 @@
 //                      4-pixel halo recomputed, not exchanged) and writes the
 //                      horizontally blurred half-resolution image
 //   composite_kernel   stages the horizontally blurred rows its tile needs in
-//                      shared memory, blurs them vertically there, samples the
-//                      result bilinearly and tonemaps the accumulation buffer
-//                      to RGBA8
+//                      shared memory, blurs them vertically there, writes the
+//                      tile's own vertically blurred half-res pixels to the
+//                      caller's second bloom buffer (the reference leaves the
+//                      finished bloom there), samples the result bilinearly
+//                      and tonemaps the accumulation buffer to RGBA8
 // Traffic per full-resolution pixel: 16 B accum read twice, 4 B half-res
-// write + ~5 B half-res read, 4 B RGBA8 write (~45 B vs ~60 B for the
-// reference's passes).  Clamp-to-edge addressing and the summation order of
+// write + ~5 B half-res read, 4 B finished-bloom write, 4 B RGBA8 write
+// (~49 B vs ~64 B for the reference's passes).  Clamp-to-edge addressing and the summation order of
 // every tap are the reference's, in exact arithmetic.
 // ---------------------------------------------------------------------------
 #include "bh_post.cuh"
@@ -78,7 +80,7 @@ bloom_h_kernel(const float4* __restrict__ acc, float4* __restrict__ hblur, int W
 
 __global__ void __launch_bounds__(CP_TX * 4)
 composite_kernel(uchar4* __restrict__ out, const float4* __restrict__ acc, const float4* __restrict__ hblur,
-                 int W, int H, int bw, int bh, PostConsts pc)
+                 float4* __restrict__ vblur, int W, int H, int bw, int bh, PostConsts pc)
 {
     __shared__ float hs[3][CP_HH][CP_HC];
     __shared__ float vs[3][CP_HR][CP_HC];
@@ -112,6 +114,12 @@ composite_kernel(uchar4* __restrict__ out, const float4* __restrict__ acc, const
                 sz = add_x(sz, mul_x(hs[2][base + k][cc], w));
             }
             vs[0][rr][cc] = sx; vs[1][rr][cc] = sy; vs[2][rr][cc] = sz;
+            // rows 1..CP_HR-2 and columns 1..CP_HC-2 are this tile's own half-res pixels
+            // (each half-res pixel belongs to exactly one tile): the reference's vertical
+            // blur output, black_hole_kernel.cu:75-84
+            const int c = hc0 + cc;
+            if (vblur && rr >= 1 && rr <= CP_HR - 2 && cc >= 1 && cc <= CP_HC - 2 && r < bh && c < bw)
+                vblur[(size_t)r * bw + c] = make_float4(sx, sy, sz, 1.f);
         }
         __syncthreads();
     }
@@ -150,7 +158,7 @@ composite_kernel(uchar4* __restrict__ out, const float4* __restrict__ acc, const
 
 }  // namespace
 
-cudaError_t bh_launch_post(uchar4* out, const float4* accum, float4* hblur, int W, int H,
+cudaError_t bh_launch_post(uchar4* out, const float4* accum, float4* hblur, float4* vblur, int W, int H,
                            const PostConsts& pc, cudaStream_t stream)
 {
     const int bw = (W + 1) / 2, bh = (H + 1) / 2;
@@ -160,6 +168,7 @@ cudaError_t bh_launch_post(uchar4* out, const float4* accum, float4* hblur, int 
         bloom_h_kernel<<<g, HB_TX, 0, stream>>>(accum, hblur, W, H, bw, bh, pc.exposure);
     }
     dim3 g2((W + CP_TX - 1) / CP_TX, (H + CP_TY - 1) / CP_TY);
-    composite_kernel<<<g2, CP_TX * 4, 0, stream>>>(out, accum, hblur, W, H, bw, bh, pc);
+    composite_kernel<<<g2, CP_TX * 4, 0, stream>>>(out, accum, hblur, pc.bloomOn ? vblur : nullptr, W, H, bw,
+                                                    bh, pc);
     return cudaGetLastError();
 }

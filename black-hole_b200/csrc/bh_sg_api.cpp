@@ -165,8 +165,8 @@ cudaError_t criticalCurve(BHSurrogate* s, const RenderParams& P0, float* crit)
     std::vector<BHProbe> rec(n);
     float3* dDirs = nullptr;
     BHProbe* dRec = nullptr;
-    cudaError_t e = cudaMalloc(&dDirs, n * sizeof(float3));
-    if (e == cudaSuccess) e = cudaMalloc(&dRec, n * sizeof(BHProbe));
+    cudaError_t e = bh_device_alloc(reinterpret_cast<void**>(&dDirs), n * sizeof(float3));
+    if (e == cudaSuccess) e = bh_device_alloc(reinterpret_cast<void**>(&dRec), n * sizeof(BHProbe));
     auto dirFor = [&](int k, float rho) {
         const float psi = 2.f * kPi * (float)k / (float)n;
         const float sx = rho * std::cos(psi), sy = rho * std::sin(psi);
@@ -206,9 +206,9 @@ cudaError_t ensureFrame(BHSurrogate* s, size_t pixels)
     if (s->heldPred) cudaFree(s->heldPred);
     s->list = nullptr; s->heldPix = nullptr; s->heldPred = nullptr; s->listCap = 0; s->heldCap = 0;
     const unsigned cap = (unsigned)want;
-    cudaError_t e = cudaMalloc(&s->list, pixels * sizeof(unsigned));
-    if (e == cudaSuccess) e = cudaMalloc(&s->heldPix, cap * sizeof(unsigned));
-    if (e == cudaSuccess) e = cudaMalloc(&s->heldPred, cap * sizeof(float4));
+    cudaError_t e = bh_device_alloc(reinterpret_cast<void**>(&s->list), pixels * sizeof(unsigned));
+    if (e == cudaSuccess) e = bh_device_alloc(reinterpret_cast<void**>(&s->heldPix), cap * sizeof(unsigned));
+    if (e == cudaSuccess) e = bh_device_alloc(reinterpret_cast<void**>(&s->heldPred), cap * sizeof(float4));
     if (e != cudaSuccess) return e;
     s->listCap = pixels;
     s->heldCap = cap;
@@ -230,15 +230,15 @@ cudaError_t bhSurrogateCreate(BHSurrogate** out, unsigned seed)
     const size_t pc = (size_t)SgLayout::count() * sizeof(float);
     cudaError_t e = cudaGetDevice(&S.device);
     if (e == cudaSuccess) e = cudaStreamCreateWithFlags(&s->stream, cudaStreamNonBlocking);
-    if (e == cudaSuccess) e = cudaMalloc(&S.params, pc);
-    if (e == cudaSuccess) e = cudaMalloc(&S.grads, pc);
-    if (e == cudaSuccess) e = cudaMalloc(&S.adamM, pc);
-    if (e == cudaSuccess) e = cudaMalloc(&S.adamV, pc);
-    if (e == cudaSuccess) e = cudaMalloc(&S.W, kWCount * 2);
-    if (e == cudaSuccess) e = cudaMalloc(&S.Wt, kWCount * 2);
-    if (e == cudaSuccess) e = cudaMalloc(&S.biasPacked, kBiasCount * sizeof(float));
-    if (e == cudaSuccess) e = cudaMalloc(&S.loss, 8 * sizeof(float));
-    if (e == cudaSuccess) e = cudaMalloc(&s->counters, 64);
+    if (e == cudaSuccess) e = bh_device_alloc(reinterpret_cast<void**>(&S.params), pc);
+    if (e == cudaSuccess) e = bh_device_alloc(reinterpret_cast<void**>(&S.grads), pc);
+    if (e == cudaSuccess) e = bh_device_alloc(reinterpret_cast<void**>(&S.adamM), pc);
+    if (e == cudaSuccess) e = bh_device_alloc(reinterpret_cast<void**>(&S.adamV), pc);
+    if (e == cudaSuccess) e = bh_device_alloc(reinterpret_cast<void**>(&S.W), kWCount * 2);
+    if (e == cudaSuccess) e = bh_device_alloc(reinterpret_cast<void**>(&S.Wt), kWCount * 2);
+    if (e == cudaSuccess) e = bh_device_alloc(reinterpret_cast<void**>(&S.biasPacked), kBiasCount * sizeof(float));
+    if (e == cudaSuccess) e = bh_device_alloc(reinterpret_cast<void**>(&S.loss), 8 * sizeof(float));
+    if (e == cudaSuccess) e = bh_device_alloc(reinterpret_cast<void**>(&s->counters), 64);
     if (e == cudaSuccess) e = bh_tc_error_word(&S.err);
     // every set-up write goes on the network's stream, ordered with the kernels that follow
     if (e == cudaSuccess) e = cudaMemsetAsync(S.W, 0, kWCount * 2, s->stream);
@@ -344,14 +344,14 @@ cudaError_t bhSurrogateGenerate(BHSurrogate* s, long long rays, int views, unsig
         if (S.dsTgt) cudaFree(S.dsTgt);
         S.dsIn = S.dsTgt = nullptr;
         S.dsN = 0;
-        if (e == cudaSuccess) e = cudaMalloc(&S.dsIn, (size_t)rays * 8 * sizeof(float));
-        if (e == cudaSuccess) e = cudaMalloc(&S.dsTgt, (size_t)rays * 8 * sizeof(float));
+        if (e == cudaSuccess) e = bh_device_alloc(reinterpret_cast<void**>(&S.dsIn), (size_t)rays * 8 * sizeof(float));
+        if (e == cudaSuccess) e = bh_device_alloc(reinterpret_cast<void**>(&S.dsTgt), (size_t)rays * 8 * sizeof(float));
         if (e != cudaSuccess) return e;
     }
     float3* dirs = nullptr;
     BHProbe* rec = nullptr;
-    if (e == cudaSuccess) e = cudaMalloc(&dirs, (size_t)R * sizeof(float3));
-    if (e == cudaSuccess) e = cudaMalloc(&rec, (size_t)R * sizeof(BHProbe));
+    if (e == cudaSuccess) e = bh_device_alloc(reinterpret_cast<void**>(&dirs), (size_t)R * sizeof(float3));
+    if (e == cudaSuccess) e = bh_device_alloc(reinterpret_cast<void**>(&rec), (size_t)R * sizeof(BHProbe));
     std::mt19937 g(seed);
     for (int v = 0; v < views && e == cudaSuccess; ++v)
     {
@@ -408,12 +408,12 @@ cudaError_t bhSurrogateTrain(BHSurrogate* s, int steps, int batch, float lr, uns
         if (s->bTgt) cudaFree(s->bTgt);
         s->bIn = s->bTgt = nullptr;
         s->bCap = 0;
-        if ((e = cudaMalloc(&s->bIn, (size_t)batch * 8 * sizeof(float))) != cudaSuccess) return e;
-        if ((e = cudaMalloc(&s->bTgt, (size_t)batch * 8 * sizeof(float))) != cudaSuccess) return e;
+        if ((e = bh_device_alloc(reinterpret_cast<void**>(&s->bIn), (size_t)batch * 8 * sizeof(float))) != cudaSuccess) return e;
+        if ((e = bh_device_alloc(reinterpret_cast<void**>(&s->bTgt), (size_t)batch * 8 * sizeof(float))) != cudaSuccess) return e;
         s->bCap = batch;
     }
     float* hist = nullptr;
-    if (steps > 0 && (e = cudaMalloc(&hist, (size_t)steps * 8 * sizeof(float))) != cudaSuccess) return e;
+    if (steps > 0 && (e = bh_device_alloc(reinterpret_cast<void**>(&hist), (size_t)steps * 8 * sizeof(float))) != cudaSuccess) return e;
     for (int it = 0; it < steps && e == cudaSuccess; ++it)
     {
         const float t = steps > 1 ? (float)it / (float)(steps - 1) : 0.f;
@@ -489,7 +489,7 @@ cudaError_t bhSurrogateRender(BHSurrogate* s, uchar4* out, float4* accum, float4
                              stream)) != cudaSuccess)
         return e;
     PostConsts pc{P.exposure, P.bloomStrength, P.bloomEnabled ? 1 : 0, P.swapRB};
-    return bh_launch_post(out, accum, bloomB, P.width, P.height, pc, stream);
+    return bh_launch_post(out, accum, bloomB, bloomA, P.width, P.height, pc, stream);
 }
 
 cudaError_t bhSurrogateFrameStats(BHSurrogate* s, BHSurrogateStats* st)

@@ -294,7 +294,7 @@ cudaError_t sg_reserve(SgState& S, int n, cudaStream_t s)
     sg_free_batch(S);
     const size_t nw = (size_t)n * kWidth;
     cudaError_t e = cudaSuccess;
-    auto take = [&](void** p, size_t bytes) { if (e == cudaSuccess) e = cudaMalloc(p, bytes); };
+    auto take = [&](void** p, size_t bytes) { if (e == cudaSuccess) e = bh_device_alloc(reinterpret_cast<void**>(p), bytes); };
     for (int l = 0; l <= kHidden; ++l) take((void**)&S.X[l], nw * 2);
     for (int l = 0; l < kHidden; ++l) take((void**)&S.Z[l], nw * 4);
     take((void**)&S.Y, (size_t)n * kOut * 4);

@@ -81,6 +81,9 @@ typedef struct BHProbe
  * (W*H float4, persistent across frames), half-resolution bloom through
  * `bloomA` / `bloomB` (ceil(W/2)*ceil(H/2) float4 each; unused when bloom is
  * off), then exposure, ACES, gamma and dither into `out` (W*H uchar4).
+ * With bloom on, the call leaves the horizontally blurred bright pass in
+ * `bloomB` and the finished (vertically blurred) bloom in `bloomA`, as the
+ * reference's passes do.
  * Replaces launchRenderPipeline, reference src/black_hole_kernel.cu:108-134. */
 cudaError_t launchRenderPipeline(uchar4* out, float4* accum, float4* bloomA, float4* bloomB,
                                  BH_PARAMS_IN p, cudaStream_t stream);
@@ -151,7 +154,8 @@ cudaError_t bhRenderPipelinePrec(uchar4* out, float4* accum, float4* bloomA, flo
 cudaError_t bhRenderAccum(float4* accum, BH_PARAMS_IN p, int precision, cudaStream_t stream);
 
 /* Post-processing alone (bloom + tonemap of an existing accumulation
- * buffer): reference src/black_hole_kernel.cu:41-103. */
+ * buffer; bloomA / bloomB filled as by launchRenderPipeline):
+ * reference src/black_hole_kernel.cu:41-103. */
 cudaError_t bhPostProcess(uchar4* out, const float4* accum, float4* bloomA, float4* bloomB,
                           BH_PARAMS_IN p, cudaStream_t stream);
 
@@ -232,9 +236,10 @@ cudaError_t bhAutotuneBatch(const BHView* views, int n, int* blocksKerr, int* bl
 #define BH_NOALLOC_MAX_HALF_PIXELS 524288
 
 /* launchRenderPipeline for callers that cannot let a library allocate device
- * memory -- a frame loop recorded inside CUDA stream capture, where cudaMalloc
- * is not allowed; a real-time loop that must never stall on the allocator; a
- * plugin whose host owns all device memory.  The caller still passes the
+ * memory -- a plugin whose host application owns all device memory and hands
+ * out only its own buffers; a real-time frame loop that must never stall on
+ * the allocator (cudaMalloc can synchronise the device).  No counterpart in
+ * the reference.  The caller still passes the
  * output (W*H uchar4) and the accumulation buffer (W*H float4, persistent);
  * the bloom intermediate and the work counter live in one fixed array inside
  * the library (256 B + BH_NOALLOC_MAX_HALF_PIXELS * 16 B = 8 MiB), which every
@@ -243,8 +248,12 @@ cudaError_t bhAutotuneBatch(const BHView* views, int n, int* blocksKerr, int* bl
  *  - Frames whose half-resolution image exceeds BH_NOALLOC_MAX_HALF_PIXELS
  *    are rejected with cudaErrorInvalidValue when bloom is on (nothing is
  *    launched); with bloom off any size is accepted.
- *  - The first call on a device looks up the array's device address; make
- *    that first call before any stream capture begins.
+ *  - The array belongs to the library's module.  Under lazy module loading
+ *    (the CUDA default) the first call on a device loads that module, which
+ *    places the 8 MiB array on the device; later calls allocate nothing.
+ *    Make that first call before any stream capture begins.
+ *  - Every call looks up the array's device address in the current context
+ *    (cudaGetSymbolAddress, which allocates nothing).
  *  - All calls on a device share the array and it keeps the last call's
  *    contents; calls that overlap on the GPU race, so serialise them (one
  *    stream, or events between streams).
@@ -255,6 +264,12 @@ cudaError_t bhRenderPipelineNoAlloc(uchar4* out, float4* accum, BH_PARAMS_IN p, 
  * of a scalar-FMA and a packed FP32x2-FMA kernel (independent chains, every
  * SM filled), timed with CUDA events (blocking). */
 double bhMeasureFp32Peak(void);
+
+/* Bytes of device memory libbh.so has allocated on `device` since it was
+ * loaded, cumulative (work-counter ring, tile-order and batch tables, graph
+ * and surrogate workspaces).  An accounting aid: a process whose only libbh
+ * calls are bhRenderPipelineNoAlloc reads 0. */
+unsigned long long bhLibraryDeviceBytes(int device);
 
 /* Library version / build string. */
 const char* bhVersion(void);

@@ -26,14 +26,25 @@ def _ptr(a):
     return a.ctypes.data_as(_vp)
 
 
+def ref_src():
+    """The reference's src/ directory: $REF_SRC, else the Makefile's default."""
+    if os.environ.get("REF_SRC"):
+        return os.environ["REF_SRC"]
+    import re
+    with open(os.path.join(HERE, "Makefile")) as fh:
+        m = re.search(r"^REF_SRC\s*\?=\s*(\S+)", fh.read(), flags=re.M)
+    return m.group(1) if m else ""
+
+
 def build(ref=None):
     """Build liboracle.so (and the reference builds when the reference tree exists)."""
     import subprocess
     subprocess.run(["make", "-s", "-C", HERE, "all"], check=True)
+    src = ref_src()
     if ref is None:
-        ref = os.path.isdir("/root/reference/src")
+        ref = bool(src) and os.path.isdir(src)
     if ref:
-        subprocess.run(["make", "-s", "-C", HERE, "ref"], check=True)
+        subprocess.run(["make", "-s", "-C", HERE, "ref", f"REF_SRC={src}"], check=True)
 
 
 class Oracle:

@@ -17,6 +17,12 @@ Fixtures (golden.npz):
                 rays of the test camera, plus the HDR shading of each ray
   pipe_<name>   launchRenderPipeline: RGBA8, accumulation and bloom buffers
   kern_<name>   launchRenderKernel: RGBA8
+
+and (config1_schwarzschild_320x180.npz) the full 320x180 Schwarzschild frame
+of the single-frame CPU workload (r = 15, elevation 15 deg, FOV 60, balanced,
+disk on at t = 0, hot spots and bloom off): launchRenderPipeline's RGBA8 and,
+per pixel, the reference probe record of the pixel's ray (outcome, class,
+steps, escape direction, transmittance, HDR).
 """
 import ctypes as C
 import os
@@ -151,6 +157,7 @@ def main():
         data[f"pipe_{name}_params"] = params_bytes(P)
         data[f"pipe_{name}_rgba"] = out
         data[f"pipe_{name}_accum"] = acc
+        data[f"pipe_{name}_bloomA"] = bA
         data[f"pipe_{name}_bloomB"] = bB
 
     # progressive accumulation from a poisoned buffer (tests/test_main.cu:596-610)
@@ -179,6 +186,28 @@ def main():
     path = os.path.join(HERE, "golden.npz")
     np.savez_compressed(path, **data)
     print(f"wrote {path} ({os.path.getsize(path) / 1024:.0f} KiB, {len(data)} arrays)")
+    config1(ref, derive)
+
+
+CONFIG1_FIELDS = ("outcome", "cls", "steps", "escDir", "trans", "hdr")
+
+
+def config1(ref, derive):
+    """The full 320x180 Schwarzschild frame: pipeline RGBA8 + per-pixel ray records.  For
+    accumMode 0 the pixel's ray is the probe ray through the pixel centre, so the
+    reference probe grid at W x H gives the frame's own rays."""
+    P = scenes.schwarzschild_320(derive)
+    out, acc, _, _ = ref.pipeline(P)
+    rec = ref.probe_grid(P, P.width, P.height)
+    # the probe's HDR is the frame's accumulation value (mode 0, one sample)
+    assert np.array_equal(rec["hdr"], acc[..., :3])
+    data = {"params": params_bytes(P), "rgba": out}
+    for k in CONFIG1_FIELDS:
+        v = rec[k]
+        data[k] = v.astype(np.int8) if k in ("outcome", "cls") else v
+    path = os.path.join(HERE, "config1_schwarzschild_320x180.npz")
+    np.savez_compressed(path, **data)
+    print(f"wrote {path} ({os.path.getsize(path) / 1024:.0f} KiB)")
 
 
 if __name__ == "__main__":

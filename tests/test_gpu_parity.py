@@ -82,9 +82,11 @@ def test_post_process_is_exact_given_the_same_hdr(cuda, name):
     s = parity.compare_rgba(f.out.cpu().numpy(), g[f"pipe_{name}_rgba"])
     print(name, s)
     assert s["max_diff"] <= 1 and s["exact_frac"] >= 0.999, s
-    if P.bloomEnabled:   # the horizontally blurred half-res image is the reference's bloomB
+    if P.bloomEnabled:   # bloomB: the horizontally blurred half-res image; bloomA: the finished bloom
         bB = f.bloomB.cpu().numpy()
         assert np.array_equal(bB[..., :3], g[f"pipe_{name}_bloomB"][..., :3])
+        bA = f.bloomA.cpu().numpy()
+        assert np.array_equal(bA, g[f"pipe_{name}_bloomA"])
 
 
 @pytest.mark.parametrize("name", ["badKN", "K9"])

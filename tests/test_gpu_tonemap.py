@@ -78,7 +78,7 @@ def _finalize(acc, P, bloom_on):
     H, W = acc.shape[:2]
     dev = acc.device
     c = acc[..., :3] * f32(P.exposure)
-    hb = None
+    hb = vb = None
     if bloom_on:
         hb, vb = _half_bloom(acc, P.exposure)
         bh, bw = vb.shape[:2]
@@ -113,7 +113,7 @@ def _finalize(acc, P, bloom_on):
         q = q[..., [2, 1, 0]]
     out = torch.full((H, W, 4), 255, dtype=torch.uint8, device=dev)
     out[..., :3] = q
-    return out, hb
+    return out, hb, vb
 
 
 def _hdr(H, W, seed):
@@ -148,11 +148,16 @@ def test_post_matches_torch_fp32_chain(cuda, W, H, bloom, swap, seed):
     P.exposure, P.bloomStrength = 1.0, 0.35
     f = Frame(W, H)
     f.accum.copy_(_hdr(H, W, seed))
+    f.bloomA.fill_(-7.0)
     f.post(P)
     torch.cuda.synchronize()
-    ref, hb = _finalize(f.accum, P, bool(bloom))
+    ref, hb, vb = _finalize(f.accum, P, bool(bloom))
     diff = (f.out.int() - ref.int()).abs()
     n_bad = int((diff > 0).any(dim=-1).sum())
     assert n_bad == 0, f"{n_bad} of {W * H} pixels differ, max {int(diff.max())}"
-    if bloom:   # bloomB holds the horizontally blurred half-res image
+    if bloom:   # bloomB: the horizontally blurred half-res image; bloomA: the finished bloom
         assert torch.equal(f.bloomB[..., :3], hb)
+        assert torch.equal(f.bloomA[..., :3], vb)
+        assert bool((f.bloomA[..., 3] == 1.0).all())
+    else:       # bloom off: the reference's passes leave both buffers alone
+        assert bool((f.bloomA == -7.0).all())

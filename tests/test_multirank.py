@@ -29,9 +29,9 @@ def _worker(rank, world, port, queue):
     try:
         import bench
         from bhrt import lib, ranks, scenes
-        times = [P.diskTime for P in bench.workload(lib.derive, rank)]
+        cams = [tuple(P.camPos.tolist()) for P in bench.workload(lib.derive, rank)]
         all_times = [None] * world
-        dist.all_gather_object(all_times, times)
+        dist.all_gather_object(all_times, cams)
         reduced = ranks.max_over_ranks([float(rank), 10.0 - rank, 3.5], world)
         views = scenes.batch_views(lib.derive, 16, 1234)
         mine = ranks.shard_views(list(range(len(views))), rank, world)
@@ -56,8 +56,9 @@ def test_two_gloo_ranks():
         p.join(timeout=120)
     assert all(p.exitcode == 0 for p in procs)
     all_times, reduced, all_shards = queue.get()
-    # distinct frames per replica (animation times are float32 in RenderParams)
-    assert all(abs(b - (a + 1.0)) < 1e-6 for a, b in zip(all_times[0], all_times[1]))
+    # distinct orbit frames per replica: no camera position rendered by both ranks
+    assert len(all_times[0]) == len(all_times[1]) == 30
+    assert not set(all_times[0]) & set(all_times[1])
     assert reduced == [1.0, 10.0, 3.5]                               # max over ranks
     assert sorted(all_shards[0] + all_shards[1]) == list(range(16))  # every view once
     assert not set(all_shards[0]) & set(all_shards[1])
@@ -69,6 +70,10 @@ def test_shard_views_bounds():
     assert ranks.shard_views(list(range(5)), 1, 3) == [1, 4]
     with pytest.raises(ValueError):
         ranks.shard_views([1], 2, 2)
+    # orbit frames: 8 ranks of 30 frames out of 300 never share a frame
+    seen = [ranks.orbit_frames_for_rank(300, 30, r) for r in range(8)]
+    flat = [k for fr in seen for k in fr]
+    assert len(flat) == len(set(flat)) == 240 and all(0 <= k < 300 for k in flat)
 
 
 def test_reference_arm_runs_on_rank_zero_only():

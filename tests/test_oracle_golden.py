@@ -36,11 +36,24 @@ def test_probe_grid_bit_exact(oracle, name):
 def test_pipeline_bit_exact(oracle, name):
     g = G.load()
     P = G.params(g[f"pipe_{name}_params"])
-    out, acc, _, bB = oracle.pipeline(P)
+    out, acc, bA, bB = oracle.pipeline(P)
     assert np.array_equal(out, g[f"pipe_{name}_rgba"])
     assert G.same_bits(acc, g[f"pipe_{name}_accum"])
     if P.bloomEnabled:
         assert G.same_bits(bB, g[f"pipe_{name}_bloomB"])
+        assert G.same_bits(bA, g[f"pipe_{name}_bloomA"])
+
+
+def test_config1_full_frame_bit_exact(oracle):
+    """The full 320x180 Schwarzschild frame: RGBA8 and every pixel's ray record."""
+    z = np.load(G.PATH.replace("golden.npz", "config1_schwarzschild_320x180.npz"))
+    P = G.params(z["params"])
+    out, acc, _, _ = oracle.pipeline(P)
+    assert np.array_equal(out, z["rgba"])
+    rec = oracle.probe_grid(P, P.width, P.height)
+    for f in ("outcome", "cls", "steps", "escDir", "trans", "hdr"):
+        assert G.same_bits(rec[f].astype(z[f].dtype), z[f]), f
+    assert G.same_bits(acc[..., :3], z["hdr"])
 
 
 def test_progressive_accumulation_bit_exact(oracle):
