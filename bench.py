@@ -64,6 +64,7 @@ sys.path.insert(0, os.path.join(ROOT, "black-hole_b200"))
 C_STEP_KERR, C_STEP_SPH, C_DISK, C_BG = 420.0, 115.0, 500.0, 250.0
 W, H = 3840, 2160
 ORBIT_FRAMES, FRAMES_PER_STEP = 300, 30
+PAIR_FRAMES = 8     # frames per scene of the 1920x1080 Kerr / Kerr-Newman pair
 L2_FLUSH_BYTES = 256 << 20
 PARAM_BYTES = 160   # RenderParams per frame, passed by value to the launch
 METRIC = "Mrays/s and 4K frame ms, plain FP32 RK4 (3840x2160 Kerr-Newman a*=0.8 q=0.3 orbit)"
@@ -377,7 +378,7 @@ def kerr_pair_leg(steps=3):
     from bhrt.abi import BHView
     from bhrt.device import Frame
     L = lib.load()
-    frames = scenes.kerr_pair_1080(lib.derive, 1920, 1080, 8)
+    frames = scenes.kerr_pair_1080(lib.derive, 1920, 1080, PAIR_FRAMES)
     fs = [Frame(1920, 1080) for _ in frames]
     views = (BHView * len(frames))()
     for i, (P, fr) in enumerate(zip(frames, fs)):
@@ -588,8 +589,8 @@ def _ray_errors(x, ref):
 
 def accuracy_leg():
     """The plain FP32 integration against the FP64 small-step integration (dPhi / 16, 16x the step
-    budget; the library's own FP64 kernel) of the bench's two scenes at 480x270, frame 0 of each,
-    per-ray records from bhProbeGrid.  FP64 at the FP32 step size against the same small-step run
+    budget; the library's own FP64 kernel) at 480x270: frame 0 of the headline orbit and frame 0 of
+    each scene of the 1920x1080 pair, per-ray records from bhProbeGrid.  FP64 at the FP32 step size against the same small-step run
     separates the method's truncation error from FP32 rounding.  Conserved quantities along the FP32
     rays: E and L_z are constants of both integrators' equations, so only the Carter constant (Binet
     first integral) and the null Hamiltonian can drift."""
@@ -597,11 +598,12 @@ def accuracy_leg():
     from bhrt.abi import BH_PREC_FP32, BH_PREC_FP64
     from bhrt.device import probe_grid
     nx, ny = 480, 270
-    frames = scenes.kerr_pair_1080(lib.derive, nx, ny, FRAMES_PER_SCENE)
-    res = {"workload": "kerr_a0.9 and kn_a-0.7_q0.4 frame 0 at 480x270 (disk, hot spots on); reference: "
-                       "FP64 with dPhi/16 and 16x maxSteps; all on the GPU",
+    frames = scenes.kerr_pair_1080(lib.derive, nx, ny, PAIR_FRAMES)
+    orbit = scenes.kn_orbit_4k(lib.derive, nx, ny, ORBIT_FRAMES, [0])[0]
+    res = {"workload": "kn_a0.8_q0.3 orbit frame 0, kerr_a0.9 and kn_a-0.7_q0.4 frame 0, at 480x270 (disk, hot "
+                       "spots on); reference: FP64 with dPhi/16 and 16x maxSteps; all on the GPU",
            "off_boundary": "rays whose reference 3x3 pixel neighbourhood holds one class"}
-    for name, P in (("kerr_a0.9", frames[0]), ("kn_a-0.7_q0.4", frames[FRAMES_PER_SCENE])):
+    for name, P in (("kn_a0.8_q0.3_orbit", orbit), ("kerr_a0.9", frames[0]), ("kn_a-0.7_q0.4", frames[PAIR_FRAMES])):
         a = probe_grid(P, nx, ny, BH_PREC_FP32)
         c = probe_grid(P, nx, ny, BH_PREC_FP64)
         Q = P.copy()
@@ -627,8 +629,9 @@ def post_leg():
     """Bloom + tonemap (bloom_h_kernel + composite_kernel through bhPostProcess) on a rendered
     3840x2160 accumulation buffer (frame 60 of the Kerr-Newman a*=0.998 sweep): 133 MB of float4,
     larger than L2, and L2 flushed before every launch.  Achieved HBM GB/s uses the fused-minimum
-    algorithmic traffic of 28 B per full-resolution pixel (16 B accumulation read, 4 B RGBA8 write,
-    ~8 B half-resolution bloom)."""
+    algorithmic traffic of 32 B per full-resolution pixel with bloom (16 B accumulation read, 4 B RGBA8
+    write, ~8 B half-resolution horizontal blur written and read, 4 B finished bloom written to
+    bloomA) and 20 B without."""
     import torch
     from bhrt import lib, scenes
     from bhrt.device import Frame
@@ -641,7 +644,8 @@ def post_leg():
     hbm = peaks.get("hbm_gbs", 6650.0)
     res = {"workload": "bhPostProcess on kn_a0.998_q0.05_r12_fov50_3840x2160 frame 60 (accum 133 MB > L2, "
                        "L2 flushed per launch)",
-           "kernels": ["bloom_h_kernel", "composite_kernel"], "algorithmic_bytes_per_px": 28.0,
+           "kernels": ["bloom_h_kernel", "composite_kernel"], "algorithmic_bytes_per_px": {"bloom_on": 32.0,
+                                                                                          "bloom_off": 20.0},
            "peak_gbs": hbm, "peak_source": "MEASURED_PEAKS.json hbm_gbs" if peaks else "fallback"}
     npx = 3840 * 2160
     for bloom in (1, 0):
@@ -657,7 +661,7 @@ def post_leg():
             torch.cuda.synchronize()
             ts.append(e0.elapsed_time(e1))
         us = float(np.median(ts)) * 1e3
-        byts = (28.0 if bloom else 20.0) * npx
+        byts = (32.0 if bloom else 20.0) * npx
         key = "bloom_on" if bloom else "bloom_off"
         res[key] = {"us_per_frame": us, "achieved_gbs": byts / (us * 1e-6) / 1e9,
                     "frac": byts / (us * 1e-6) / 1e9 / hbm}

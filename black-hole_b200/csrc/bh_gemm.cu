@@ -64,7 +64,8 @@ tc_gemm_kernel(const __grid_constant__ CUtensorMap tA, const __grid_constant__ C
 
     if (threadIdx.x == 0)
     {   // TMA producer
-        for (int kb = 0; kb < kBlocks; ++kb)
+        int issued = 0;
+        for (int kb = 0; kb < kBlocks; ++kb, ++issued)
         {
             const int s = kb % kStages;
             if (kb >= kStages && !mbar_wait(&empty[s], ((kb / kStages) - 1) & 1, err)) break;
@@ -73,6 +74,10 @@ tc_gemm_kernel(const __grid_constant__ CUtensorMap tA, const __grid_constant__ C
             tma_load_2d(st, &tA, &full[s], (kb0 + kb) * 64, m0);
             tma_load_2d(st + kATileBytes, &tB, &full[s], (kb0 + kb) * 64, n0);
         }
+        // the CTA leaves only once its copies have landed, also after a timed-out wait
+        // (bounded waits; on the normal path these phases are complete already)
+        for (int kb = issued > kStages ? issued - kStages : 0; kb < issued; ++kb)
+            if (!mbar_wait(&full[kb % kStages], (kb / kStages) & 1, err)) break;
     }
     else if (threadIdx.x == 32)
     {   // MMA issuer

@@ -416,7 +416,7 @@ struct KerrEval
 template <class R>
 struct KerrConsts
 {
-    R E, Lz, aE, c1, fourE;   // c1 = E a^2 - a Lz, so P = E r^2 + c1
+    R E, Lz, aE, c1, twoE;    // c1 = E a^2 - a Lz, so P = E r^2 + c1
 };
 
 // per lane: x >= thr ? a : b
@@ -469,14 +469,14 @@ BH_DEV KerrEval<V> kerr_rhs(const CamFrame<S>& F, const KerrConsts<V>& k, V r, V
     const V Dpr = vmul(Del, pr);
     KerrEval<V> o;
     o.K = vfma(Dpr, pr, vfma(pth, pth, W));                                // Delta pr^2 + pth^2 + W
-    const V dDel = vadd(rm2M, r);                                          // dDelta/dr = 2 (r - M)
-    const V Wr = vmul(PiD, vfma(PiD, dDel, vneg(vmul(k.fourE, r))));       // dW/dr = -P/D (dP - P/D dDelta)
+    const V rmM = vsub(r, M);                                              // dDelta/dr / 2
+    const V Wrh = vmul(PiD, vfma(PiD, rmM, vneg(vmul(k.twoE, r))));        // dW/dr / 2 = -P/D (dP - P/D dDelta) / 2
     const V KiS = vmul(o.K, iS);
     o.d.r = vmul(Dpr, iS);
     o.d.th = vmul(pth, iS);
     o.d.ph = vmul(vfma(lane<V>(F.a), PiD, vfma(k.Lz, is2, vneg(k.aE))), iS);
     // dpr = -(dH/dr) = (r K / Sigma - (dDelta pr^2 + dW/dr) / 2) / Sigma
-    o.d.pr = vmul(iS, vfma(lane<V>((S)-0.5f), vfma(vmul(dDel, pr), pr, Wr), vmul(r, KiS)));
+    o.d.pr = vmul(iS, vfma(vneg(vmul(rmM, pr)), pr, vfma(r, KiS, vneg(Wrh))));
     // dpth = -(dH/dth) = cos (B (Lz / s^2 + a E) - a^2 s K / Sigma) / Sigma
     o.d.pth = vmul(vmul(c, iS), vfma(B, vfma(k.Lz, is2, k.aE), vneg(vmul(vmul(a2, s), KiS))));
     o.Pp = Pp;
@@ -529,7 +529,7 @@ static __device__ __noinline__ KerrStep64 kerr_rk4_fp64(const CamFrame<double>& 
                                                         float th0, float ph0, float pr0, float pth0, float hf)
 {
     const double E = Ef, Lz = Lzf, h = hf;
-    const KerrConsts<double> k{E, Lz, F.a * E, E * F.a2 - F.a * Lz, 4.0 * E};
+    const KerrConsts<double> k{E, Lz, F.a * E, E * F.a2 - F.a * Lz, 2.0 * E};
     double r = r0, th = th0, ph = ph0, pr = pr0, pth = pth0, s, c;
     sincos(th, &s, &c);
     KerrDeriv<double> d1 = kerr_rhs(F, k, r, s, c, pr, pth).d;
@@ -584,6 +584,7 @@ struct KerrRay
     float trans, maxHviol;
     int step;
     bool horizon, escaped, useDeriv;
+    bool prevCart;          // prevPos holds (x, y, z); else (r sin th, y, ph) of the last point
     DiskTally tally;
     double Q0;
 
@@ -626,7 +627,7 @@ struct KerrRay
             pth = xmul(dtc, F.sqS);
             r = F.r0; th = F.th0; ph = F.ph0;
         }
-        k.E = E; k.Lz = Lz; k.aE = F.a * E; k.c1 = E * F.a2 - F.a * Lz; k.fourE = R(4) * E;
+        k.E = E; k.Lz = Lz; k.aE = F.a * E; k.c1 = E * F.a2 - F.a * Lz; k.twoE = R(2) * E;
         sincos_theta(th, s, c);
         KerrEval<R> ev = kerr_rhs(F, k, r, s, c, pr, pth);
         d1 = ev.d;
@@ -634,6 +635,7 @@ struct KerrRay
 
         tFlight = R(0);
         prevPos = tof3(P.camPos);
+        prevCart = true;
         accum = v3(0.f, 0.f, 0.f);
         trans = 1.f;
         maxHviol = 0.f;
@@ -676,7 +678,10 @@ struct KerrRay
 
         // adaptive affine step (reference src/trace.cuh:793-809)
         const R ang = abs_p(d1.th) + abs_p(d1.ph);
-        R h = rcp_p(abs_p(d1.r) * rcp_p(F.k8dPhi * max_p(r - F.rFloor, R(0.02f))) + ang * F.i22dPhi + R(1e-5f));
+        // h = 1 / (|dr| / kq + ang / (2.2 dPhi) + 1e-5) with kq = 8 dPhi max(r - rFloor, 0.02),
+        // formed as one quotient kq / (kq (ang / (2.2 dPhi) + 1e-5) + |dr|)
+        const R kq = F.k8dPhi * max_p(r - F.rFloor, R(0.02f));
+        R h = kq * rcp_p(kq * (ang * F.i22dPhi + R(1e-5f)) + abs_p(d1.r));
         if (r < F.rPh15) h *= R(0.55f);
         R spd = abs_p(d1.r) + r * ang + R(1e-6f);
         R capLen;
@@ -734,19 +739,49 @@ struct KerrRay
             tFlight += h * abs_p(dtdl);
         }
         if (STATS) equator_crossing(P, h, rS, thS, drS, dthS);
-        if (P.diskOn)
-        {
-            R sp, cp;
-            sincos_fast(ph, sp, cp);
-            R rs = r * s, px, pz;
-            mul2_p(rs, -rs, cp, sp, px, pz);
-            f3 pos = v3((float)px, (float)(r * c), (float)pz);
-            if (trans > 0.01f)
-                disk_segment<STATS>(P, (float)k.E, (float)k.Lz, prevPos, pos, (float)(F.diskTime - tFlight),
-                                    accum, trans, tally);
-            prevPos = pos;
-        }
+        if (P.diskOn) disk_chord(P, F);
         return false;
+    }
+
+    // Cartesian point (kerrToCart, reference src/trace.cuh:665-671) from r sin th,
+    // r cos th and the azimuth.
+    BH_DEV static f3 cart(R rs, float y, R phi)
+    {
+        R sp, cp, px, pz;
+        sincos_fast(phi, sp, cp);
+        mul2_p(rs, -rs, cp, sp, px, pz);
+        return v3((float)px, y, (float)pz);
+    }
+
+    // The disk chord from the previous point to the current one (reference
+    // src/trace.cuh:853-866).  The chord's first test in disk_segment is the
+    // vertical slab cull on the two end heights; most steps of most rays are
+    // culled there, so for FP32 rays the azimuthal part of the Cartesian
+    // point (a sincos and two products) is formed only when a chord can
+    // reach the slab: a culled point keeps (r sin th, y, ph) and becomes
+    // Cartesian only if the next chord needs it.  The values, and so the
+    // chord, are the same bits as forming every point.
+    BH_DEV void disk_chord(const TraceParams& P, const CamFrame<R>& F)
+    {
+        const R rs = r * s;
+        const float y = (float)(r * c);
+        if constexpr (std::is_same<R, float>::value)
+        {
+            const float maxH = 0.16f * P.diskOuter;
+            if ((prevPos.y > maxH && y > maxH) || (prevPos.y < -maxH && y < -maxH))
+            {   // culled: keep the point in polar form
+                prevPos = v3((float)rs, y, (float)ph);
+                prevCart = false;
+                return;
+            }
+            if (!prevCart) prevPos = cart((R)prevPos.x, prevPos.y, (R)prevPos.z);
+        }
+        const f3 pos = cart(rs, y, ph);
+        if (trans > 0.01f)
+            disk_segment<STATS>(P, (float)k.E, (float)k.Lz, prevPos, pos, (float)(F.diskTime - tFlight), accum,
+                                trans, tally);
+        prevPos = pos;
+        prevCart = true;
     }
 
     // Equatorial crossing inside the last step: bisection of the cubic Hermite
@@ -822,14 +857,15 @@ __device__ __noinline__ bool KerrRay<R, STATS, MIXED>::polar_passage_fp64(const 
         const CamFrame<double>& D = P.cd;
         KerrRay<double, STATS, false> d;
         const double E = k.E, Lz = k.Lz;
-        d.k = KerrConsts<double>{E, Lz, D.a * E, E * D.a2 - D.a * Lz, 4.0 * E};
+        d.k = KerrConsts<double>{E, Lz, D.a * E, E * D.a2 - D.a * Lz, 2.0 * E};
         d.r = r; d.th = th; d.ph = ph; d.pr = pr; d.pth = pth;
         sincos_theta(d.th, d.s, d.c);
         KerrEval<double> ev = kerr_rhs(D, d.k, d.r, d.s, d.c, d.pr, d.pth);
         d.d1 = ev.d;
         d.K1 = ev.K;
         d.tFlight = tFlight;
-        d.prevPos = prevPos; d.accum = accum; d.trans = trans; d.maxHviol = maxHviol;
+        if (!prevCart) { prevPos = cart((R)prevPos.x, prevPos.y, (R)prevPos.z); prevCart = true; }
+        d.prevPos = prevPos; d.prevCart = true; d.accum = accum; d.trans = trans; d.maxHviol = maxHviol;
         d.step = step; d.horizon = horizon; d.escaped = escaped; d.useDeriv = useDeriv;
         if (STATS) { d.tally = tally; d.Q0 = Q0; }
         bool done = false;
@@ -838,7 +874,7 @@ __device__ __noinline__ bool KerrRay<R, STATS, MIXED>::polar_passage_fp64(const 
             if (abs_p(d.s) >= 0.0625) break;
         r = (R)d.r; th = (R)d.th; ph = (R)d.ph; pr = (R)d.pr; pth = (R)d.pth;
         tFlight = (R)d.tFlight;
-        prevPos = d.prevPos; accum = d.accum; trans = d.trans; maxHviol = d.maxHviol;
+        prevPos = d.prevPos; prevCart = true; accum = d.accum; trans = d.trans; maxHviol = d.maxHviol;
         step = d.step; horizon = d.horizon; escaped = d.escaped; useDeriv = d.useDeriv;
         if (STATS) tally = d.tally;
         if (done && escaped && useDeriv && step >= P.maxSteps)

@@ -182,6 +182,9 @@ BH_DEV float2 vmul(float2 a, float2 b)  { return __fmul2_rn(a, b); }
 BH_DEV float  vadd(float a, float b)    { return __fadd_rn(a, b); }
 BH_DEV double vadd(double a, double b)  { return __dadd_rn(a, b); }
 BH_DEV float2 vadd(float2 a, float2 b)  { return __fadd2_rn(a, b); }
+BH_DEV float  vsub(float a, float b)    { return __fsub_rn(a, b); }
+BH_DEV double vsub(double a, double b)  { return __dsub_rn(a, b); }
+BH_DEV float2 vsub(float2 a, float2 b)  { return make_float2(__fsub_rn(a.x, b.x), __fsub_rn(a.y, b.y)); }
 BH_DEV float  vneg(float a)  { return -a; }
 BH_DEV double vneg(double a) { return -a; }
 BH_DEV float2 vneg(float2 a) { return make_float2(-a.x, -a.y); }

@@ -50,7 +50,7 @@ constexpr uint32_t kSmemBytes = 2 * kTileBytes + kRing * kChunkBytes + 1024;
 
 struct Bars
 {
-    uint64_t full[kRing], empty[kRing], aReady[2], accFull[2];
+    uint64_t full[kRing], empty[kRing], aReady[2], accFull[2], done;
     uint32_t tmem;
 };
 
@@ -193,6 +193,7 @@ sg_infer_kernel(const __grid_constant__ CUtensorMap tW, const __grid_constant__ 
     {
         for (int s = 0; s < kRing; ++s) { mbar_init(&B.full[s], 1); mbar_init(&B.empty[s], 1); }
         for (int g = 0; g < 2; ++g) { mbar_init(&B.aReady[g], 512); mbar_init(&B.accFull[g], 1); }
+        mbar_init(&B.done, 1);
         fence_barrier_init();
     }
     if (warp == kProducerWarp)
@@ -228,8 +229,9 @@ sg_infer_kernel(const __grid_constant__ CUtensorMap tW, const __grid_constant__ 
                             if (l < kHidden) tma_load_2d_pair(dst, &tW, leaderFull, kb * 64, l * 256 + (int)rank * 128);
                             else tma_load_2d_pair(dst, &tH, leaderFull, kb * 64, (int)rank * kOut);
                         }
-            // drain: the last loads must land before the pair may exit
-            if (rank == 0 && ok && q > 0)
+            // drain: the last loads (of both CTAs, which complete on the leader's barriers)
+            // must land before the pair may exit -- also after a timed-out wait
+            if (rank == 0 && q > 0)
                 for (uint32_t k = (q > kRing ? q - kRing : 0); k < q; ++k)
                     if (!mbar_wait_cluster(&B.full[k % kRing], (k / kRing) & 1, err)) break;
         }
@@ -265,7 +267,11 @@ sg_infer_kernel(const __grid_constant__ CUtensorMap tW, const __grid_constant__ 
                         }
                         mma_commit_pair(&B.accFull[g]);
                     }
+            // every MMA issued has completed before the pair frees its TMEM (also
+            // after a timed-out wait); the commit arrives on both CTAs' barriers
+            mma_commit_pair(&B.done);
         }
+        if (lane == 0) mbar_wait_cluster(&B.done, 0, err);
     }
     else
     {   // ---- epilogue groups ----

@@ -71,9 +71,14 @@ template <class Ray, bool STATS>
 BH_DEV void shade_slot(const TraceParams& P, const PackedRay<typename Ray::Real>& q, const PackedStats* qs)
 {
     const bool horizon = (q.key & kRayHorizon) != 0u, escaped = (q.key & kRayEscaped) != 0u;
-    const unsigned key = q.key & kRayKeyMask;
+    const unsigned key = q.key & kRayKeyMask;     // pixel index; the list position in anchor mode
     int px = 0, py = 0;
-    if (!P.dirs) { py = (int)(key / (unsigned)P.W); px = (int)(key - (unsigned)py * (unsigned)P.W); }
+    if (!P.dirs)
+    {
+        const unsigned pix = (P.outMode == BH_OUT_ANCHOR) ? __ldg(P.pixList + key) : key;
+        py = (int)(pix / (unsigned)P.W);
+        px = (int)(pix - (unsigned)py * (unsigned)P.W);
+    }
     f3 esc = v3(0.f, 0.f, 0.f);
     if (escaped)
         esc = (q.key & kRayUseState) ? Ray::escape_dir(P, q) : ray_direction(P, key, px, py);
@@ -106,6 +111,17 @@ BH_DEV void shade_slot(const TraceParams& P, const PackedRay<typename Ray::Real>
     case BH_OUT_HDR:
         reinterpret_cast<float4*>(P.out)[key] = make_float4(hdr.x, hdr.y, hdr.z, 1.f);
         break;
+    case BH_OUT_ANCHOR:
+    {
+        BHAnchor a;
+        a.escDir = make_float3(esc.x, esc.y, esc.z);
+        const bool disk = q.trans < 1.f || q.acc[0] > 0.f || q.acc[1] > 0.f || q.acc[2] > 0.f;
+        a.flags = (escaped ? BH_ANCHOR_ESCAPED : 0u) | (horizon ? BH_ANCHOR_HORIZON : 0u) | (disk ? BH_ANCHOR_DISK : 0u);
+        a.hdr = make_float3(hdr.x, hdr.y, hdr.z);
+        a.trans = q.trans;
+        reinterpret_cast<BHAnchor*>(P.out)[key] = a;
+        break;
+    }
     default:
     {
         BHProbe o;
@@ -187,7 +203,8 @@ trace_kernel(const __grid_constant__ TraceParams P)
                     if (inFrame)
                     {
                         rid = id;
-                        key = P.dirs ? id : (unsigned)py * (unsigned)P.W + (unsigned)px;
+                        key = (P.dirs || P.outMode == BH_OUT_ANCHOR) ? id
+                                                                     : (unsigned)py * (unsigned)P.W + (unsigned)px;
                         int st = ray.init(P, ray_direction(P, id, px, py));
                         live = (st == RAY_LIVE);
                         fin = (st == RAY_DONE);
@@ -262,7 +279,7 @@ BH_DEV void trace_tile(const TraceParams& P, unsigned tile, unsigned lane, unsig
     unsigned key = 0;
     if (inFrame)
     {
-        key = (unsigned)py * (unsigned)P.W + (unsigned)px;
+        key = (P.outMode == BH_OUT_ANCHOR) ? rid : (unsigned)py * (unsigned)P.W + (unsigned)px;
         const int st = ray.init(P, ray_direction(P, rid, px, py));
         live = (st == RAY_LIVE);
         fin = (st == RAY_DONE);

@@ -16,7 +16,19 @@ enum BhOutMode
     BH_OUT_RGBA = 1,    // finalise straight to uchar4 (no bloom): launchRenderKernel
     BH_OUT_HDR = 2,     // write the HDR sample as float4
     BH_OUT_PROBE = 3,   // write a BHProbe record per ray
+    BH_OUT_ANCHOR = 4,  // pixel-list rays: write a BHAnchor record per list entry
 };
+
+// Compact record of one traced pixel of a list (BH_OUT_ANCHOR), indexed by the
+// list position: the escape direction (world), outcome flags and the HDR sample.
+struct BHAnchor
+{
+    float3 escDir;
+    unsigned flags;     // BH_ANCHOR_*
+    float3 hdr;
+    float trans;
+};
+enum { BH_ANCHOR_ESCAPED = 1u, BH_ANCHOR_HORIZON = 2u, BH_ANCHOR_DISK = 4u };
 
 // Camera-frame quantities shared by every ray of a view, in the integration
 // precision T.  They are the per-ray prologue of the reference integrators

@@ -16,11 +16,13 @@ radiance and 8-bit output):
   4  32 of the 256 random views of seed 1234 (every 8th), rendered in one
      bhRenderBatch call with the other 224: the CPU oracle, live.
 
-Bars (measured levels, asserted per configuration): outcome class identical
-off the class boundaries; escape directions within 1e-4 rad on >= 99 % of
-off-boundary escaped rays; RGBA8 within +-1 LSB on >= 99.5 % of pixels; HDR
-within 1e-3 relative (floor 1e-3) on the off-boundary fraction stated in
-HDR_1E3 below.  The HDR misses are rays that graze a sub-pixel star core or a
+Bars (asserted per configuration at the levels measured on B200): outcome
+class identical off the class boundaries; escape directions within 1e-4 rad
+on >= 99.9 % of off-boundary escaped rays (config 1: 100 %); RGBA8 within
++-1 LSB on >= 99.95 % of pixels; HDR within 1e-3 relative (floor 1e-3) on the
+off-boundary fraction stated in HDR_1E3 below (measured: config 1 99.83 %,
+config 2 99.67 / 99.65 %, config 3 99.31-99.65 %, config 4 99.02 % in the
+worst of the 32 views, 99.6 % on average).  The HDR misses are rays that graze a sub-pixel star core or a
 disk-noise cell edge, where a ~1e-7 rad difference in direction, from
 different (correctly rounded vs hardware) sin/cos and reciprocal roundings,
 moves the sample across a steep texture edge.
@@ -38,7 +40,7 @@ from bhrt.abi import BH_PREC_FP32, BH_PREC_FP64, BH_PREC_MIXED, PROBE_DTYPE
 pytestmark = pytest.mark.gpu
 
 # off-boundary fraction of pixels whose HDR is within 1e-3 relative of the oracle's
-HDR_1E3 = {"config1": 0.995, "config2": 0.99, "config3": 0.99, "config4": 0.99}
+HDR_1E3 = {"config1": 0.998, "config2": 0.996, "config3": 0.99, "config4_worst": 0.985, "config4_mean": 0.995}
 
 
 def _hdr_frac(got, ref, mask):
@@ -71,9 +73,9 @@ def test_config1_schwarzschild_320x180_full_frame(cuda):
     inner = ~parity.boundary_mask(ref["cls"])
     hf = _hdr_frac(acc, ref["hdr"], inner)
     print("config1", s, st, "frame hdr within 1e-3:", hf)
-    assert s["alpha_ok"] and s["lsb1_frac"] >= 0.995, s
+    assert s["alpha_ok"] and s["lsb1_frac"] >= 0.9995, s
     assert st["cls_mismatch_inner"] == 0, st
-    assert st["esc_frac_1e4"] >= 0.99, st
+    assert st["esc_frac_1e4"] == 1.0, st
     assert st["hdr_frac_1e3"] >= HDR_1E3["config1"] and hf >= HDR_1E3["config1"], (st, hf)
 
 
@@ -90,9 +92,9 @@ def test_config2_full_hd_frame(cuda, oracle, k):
     inner = ~parity.boundary_mask(ref_rays["cls"])
     hf = _hdr_frac(acc, ref_hdr, inner)
     print(f"config2 frame {k}", s, st, "frame hdr within 1e-3:", hf)
-    assert s["alpha_ok"] and s["lsb1_frac"] >= 0.995, s
+    assert s["alpha_ok"] and s["lsb1_frac"] >= 0.9995, s
     assert st["cls_mismatch_inner"] == 0, st
-    assert st["esc_frac_1e4"] >= 0.99, st
+    assert st["esc_frac_1e4"] >= 0.999, st
     assert hf >= HDR_1E3["config2"], hf
 
 
@@ -117,15 +119,16 @@ def test_config3_sweep_frame_480x270(cuda, oracle, fid):
           f"fp64-vs-oracle64 {s64}\n  fp32-vs-oracle64 {f32_vs_64}")
     for st in (s32, smx, s64):
         assert st["cls_mismatch_inner"] <= max(2, int(1e-4 * nx * ny)), st
-    assert s64["esc_frac_1e4"] >= 0.995, s64
-    # mixed: within 1e-4 rad of the FP64 integration on >= 99 % of rays at every
-    # elevation, and closer to it than plain FP32
-    assert smx["esc_frac_1e4"] >= 0.99, smx
+    assert s64["esc_frac_1e4"] >= 0.999, s64
+    # mixed: within 1e-4 rad of the FP64 integration on >= 99.9 % of rays at every
+    # elevation (measured 99.92 % at 89 deg), and closer to it than plain FP32
+    # (measured 98.5 % at 89 deg: the polar passages)
+    assert smx["esc_frac_1e4"] >= 0.999, smx
     assert smx["esc_frac_1e4"] >= f32_vs_64["esc_frac_1e4"], (smx, f32_vs_64)
-    # FP32 against the reference's FP32 method: near the spin axis both FP32
-    # integrations are ill-conditioned (polar passages), so the bar is 98 % there
-    assert s32["esc_frac_1e4"] >= (0.99 if el < 80 else 0.98), s32
-    assert s32["hdr_frac_1e3"] >= (HDR_1E3["config3"] if el < 80 else 0.98), s32
+    # FP32 against the reference's own FP32 method (both start from the same rounded
+    # initial state, so they agree even where both drift from FP64)
+    assert s32["esc_frac_1e4"] >= 0.999, s32
+    assert s32["hdr_frac_1e3"] >= HDR_1E3["config3"], s32
 
 
 def test_config4_batch_views_against_oracle(cuda, oracle):
@@ -149,7 +152,7 @@ def test_config4_batch_views_against_oracle(cuda, oracle):
     sp = C.c_void_p(torch.cuda.current_stream().cuda_stream)
     lib.check(L.bhRenderBatch(arr, len(views), sp), "bhRenderBatch")
     torch.cuda.synchronize()
-    worst_lsb, worst_hdr = 1.0, 1.0
+    worst_lsb, worst_hdr, hdrs = 1.0, 1.0, []
     for i in range(0, len(views), 8):
         P = views[i]
         ref_hdr, ref_rays = oracle.render_hdr(P, rays=True)
@@ -160,7 +163,9 @@ def test_config4_batch_views_against_oracle(cuda, oracle):
         inner = ~parity.boundary_mask(ref_rays["cls"])
         hf = _hdr_frac(acc, ref_hdr, inner)
         print(f"config4 view {i} {P.width}x{P.height} model {P.model}", s, "hdr within 1e-3:", hf)
-        assert s["alpha_ok"] and s["lsb1_frac"] >= 0.995, (i, s)
+        assert s["alpha_ok"] and s["lsb1_frac"] >= 0.9995, (i, s)
         worst_lsb, worst_hdr = min(worst_lsb, s["lsb1_frac"]), min(worst_hdr, hf)
-    print("config4 worst view: rgba within 1 LSB", worst_lsb, "hdr within 1e-3", worst_hdr)
-    assert worst_hdr >= HDR_1E3["config4"], worst_hdr
+        hdrs.append(hf)
+    print("config4 worst view: rgba within 1 LSB", worst_lsb, "hdr within 1e-3", worst_hdr, "mean", np.mean(hdrs))
+    assert worst_hdr >= HDR_1E3["config4_worst"], worst_hdr
+    assert np.mean(hdrs) >= HDR_1E3["config4_mean"], np.mean(hdrs)
