@@ -469,10 +469,16 @@ def surrogate_leg():
         sur(scene(0))                                   # first frame: critical curve by RK4 bisection
         torch.cuda.synchronize()
         t_first = time.perf_counter() - t0
-        gates = {"strict": (0.95, 0.95, 0.02, 256), "permissive": (0.5, 0.0, 0.02, 256)}
+        # (anchor stride, network cell gate, minProb, minConf, critBand, held-out stride)
+        gates = {"anchored_strict": (4, 1, 0.95, 0.95, 0.02, 256),
+                 "anchored_no_network": (4, 0, 0.95, 0.95, 0.02, 256),
+                 "network_strict": (0, 1, 0.95, 0.95, 0.02, 256),
+                 "network_permissive": (0, 1, 0.5, 0.0, 0.02, 256)}
         res = {}
         plain_ms = []
-        for gname, g in gates.items():
+        for gname, gg in gates.items():
+            lib.check(L.bhSurrogateSetAnchors(h, gg[0], gg[1], C.c_float(1e-4), C.c_float(0.5)), "anchors")
+            g = gg[2:]
             lib.check(L.bhSurrogateSetGate(h, C.c_float(g[0]), C.c_float(g[1]), C.c_float(g[2]), g[3]), "gate")
             sur_ms, within, rk4, held, held_bad = [], [], [], 0, 0
             for k in SG_FRAMES:
@@ -480,17 +486,19 @@ def surrogate_leg():
                 fa.pipeline(P)
                 sur(P)
                 torch.cuda.synchronize()
-                if gname == "strict":
+                if gname == "anchored_strict":
                     plain_ms.append(timed(lambda: fa.pipeline(P)))
                 sur_ms.append(timed(lambda: sur(P)))
                 d = (fa.out[..., :3].int() - fb.out[..., :3].int()).abs().amax(dim=-1)
                 within.append(float((d <= 1).float().mean()))
-                st = np.zeros(6, dtype=np.uint32)
+                st = np.zeros(12, dtype=np.uint32)
                 lib.check(L.bhSurrogateFrameStats(h, st.ctypes.data_as(C.c_void_p)), "stats")
                 rk4.append(float(st[1]) / (SG_W * SG_H))
                 held += int(st[2])
                 held_bad += int(st[3])
-            res[gname] = {"gate": {"min_prob": g[0], "min_conf": g[1], "crit_band": g[2], "held_stride": g[3]},
+            res[gname] = {"gate": {"anchor_stride": gg[0], "network_cell_gate": bool(gg[1]), "min_prob": g[0],
+                                   "min_conf": g[1], "crit_band": g[2], "held_stride": g[3]},
+                          "interpolated_frac": float(st[7]) / (SG_W * SG_H),
                           "frame_ms": float(np.median(sur_ms)),
                           "px_within_1lsb": float(np.min(within)),
                           "rk4_pixel_frac": float(np.mean(rk4)),

@@ -36,6 +36,8 @@ def named(name, frame, width, height):
         return scenes.kerr_pair_1080(d, width or 1920, height or 1080)[frame % 16]
     if name == "kn4k":
         return scenes.kn_sweep_4k(d, width or 3840, height or 2160, frame_ids=[frame % 120])[0]
+    if name == "orbit4k":
+        return scenes.kn_orbit_4k(d, width or 3840, height or 2160, 300, [frame % 300])[0]
     if name == "batch":
         v = scenes.batch_views(d)[frame % 256]
         return v
@@ -119,7 +121,7 @@ def main(argv=None):
     ap = argparse.ArgumentParser(description=__doc__, formatter_class=argparse.RawDescriptionHelpFormatter)
     ap.add_argument("cmd", choices=["render", "sweep", "batch", "mlp", "info"])
     ap.add_argument("--rays", type=int, default=3840 * 2160)
-    ap.add_argument("--scene", default=None, help="schw320 | kerr1080 | kn1080 | pair1080 | kn4k | batch")
+    ap.add_argument("--scene", default=None, help="schw320 | kerr1080 | kn1080 | pair1080 | kn4k | orbit4k | batch")
     ap.add_argument("--frame", type=int, default=0)
     ap.add_argument("--frames", type=int, default=120)
     ap.add_argument("--step", type=int, default=1)

@@ -62,6 +62,7 @@ _SIGNATURES = {
     "bhSurrogateRender": (_int, [_vp, _vp, _vp, _vp, _vp, _P, _vp]),
     "bhSurrogateFrameStats": (_int, [_vp, _vp]),
     "bhSurrogateSetGate": (_int, [_vp, C.c_float, C.c_float, C.c_float, _int]),
+    "bhSurrogateSetAnchors": (_int, [_vp, _int, _int, C.c_float, C.c_float]),
     "bhVersion": (C.c_char_p, []),
 }
 

@@ -36,6 +36,15 @@
 
 enum { RAY_SKIP = 0, RAY_LIVE = 1, RAY_DONE = 2 };
 
+// MIXED precision: the polar cap |sin th| < kPolarCap (0.9 deg) inside which a
+// Kerr-family ray carries an FP64 state (KerrRay::polar_passage_fp64).  Measured
+// on the 4K near-extremal sweep at 89 deg elevation (480x270, escape directions
+// within 1e-4 rad of the FP64 integration): no cap 98.6 %, 1/64 99.79 %, 1/32
+// 99.93 %, 1/16 99.93 %; frame time against FP32 at 0 / 45 / 89 deg: 1.5 / 1.6 /
+// 2.4x at 1/64, 2.1 / 2.3 / 3.2x at 1/32, 2.8 / 3.2 / 4.0x at 1/16 (a warp
+// waits for its lanes' FP64 passages).
+constexpr float kPolarCap = 1.0f / 64.0f;
+
 // A finished ray as it waits for shading: outcome flags, the radiance gathered
 // from the disk, and the six state values from which the escape direction is
 // rebuilt at shading time (so the finishing lane only stores, and the
@@ -105,14 +114,14 @@ BH_DEV void sincos_theta(float x, float& s, float& c)
     __sincosf(x, &s, &c);
     if (fabsf(s) < 0.0625f) sincos_polar(x, s, c);
 }
-BH_DEV void sincos_theta(double x, double& s, double& c) { sincos(x, &s, &c); }
+BH_DEV void sincos_theta(double x, double& s, double& c) { sincos_cap(x, s, c); }
 
 // RK4 stage angles: the same pole-accurate pair.  (A plain MUFU sine has only
 // absolute accuracy, ~4e-7: near the poles the 1/sin^2 terms of the stages then
 // carry ~1e-5 relative error, enough to move escape directions by ~1e-4 rad
 // for cameras within a few degrees of the spin axis.)
 BH_DEV void sincos_stage(float x, float& s, float& c) { sincos_theta(x, s, c); }
-BH_DEV void sincos_stage(double x, double& s, double& c) { sincos(x, &s, &c); }
+BH_DEV void sincos_stage(double x, double& s, double& c) { sincos_cap(x, s, c); }
 
 // Cubic Hermite interpolant on a step: value at fraction t of the step of
 // length h, from end values y0, y1 and derivatives d0, d1 (per unit parameter).
@@ -555,7 +564,7 @@ static __device__ __noinline__ KerrStep64 kerr_rk4_fp64(const CamFrame<double>& 
 // position), whole steps in FP64 at radial turning points (p_r would change
 // sign within the step -- for near-extremal holes this includes periapses a
 // few percent outside the horizon), FP64 state and steps through every polar
-// passage (|sin th| < 1/16, below), and FP64 bisection of the equatorial
+// passage (|sin th| < kPolarCap, below), and FP64 bisection of the equatorial
 // crossing.  (FP64 steps over the whole final horizon approach were measured
 // to cost 70 % more time for no accuracy gain, and are not taken.)
 //
@@ -567,8 +576,8 @@ static __device__ __noinline__ KerrStep64 kerr_rk4_fp64(const CamFrame<double>& 
 // ~1e-3 relative, and the escape direction by ~1e-4 rad).  FP64 arithmetic
 // inside each step does not help while the state is rounded back to FP32
 // between steps; what does is to carry an FP64 state from the step that enters
-// the cap |sin th| < 1/16 to the step that leaves it, so that is what MIXED
-// does (polar_passage_fp64).
+// the cap |sin th| < kPolarCap to the step that leaves it, so that is what
+// MIXED does (polar_passage_fp64).
 template <class R, bool STATS, bool MIXED = false>
 struct KerrRay
 {
@@ -695,7 +704,7 @@ struct KerrRay
         R dl0 = R(0), dl1 = R(0), dl2 = R(0);                 // the final stage's derivative
         if constexpr (MIXED)
         {
-            if (abs_p(s) < R(0.0625f)) return polar_passage_fp64(P);
+            if (abs_p(s) < R(kPolarCap)) return polar_passage_fp64(P);
             if (abs_p(pr) < h * abs_p(d1.pr))
             {
                 KerrStep64 o = kerr_rk4_fp64(P.cd, k.E, k.Lz, r, th, ph, pr, pth, h);
@@ -744,13 +753,15 @@ struct KerrRay
     }
 
     // Cartesian point (kerrToCart, reference src/trace.cuh:665-671) from r sin th,
-    // r cos th and the azimuth.
+    // r cos th and the azimuth.  The point feeds the float disk shading, so an
+    // FP64 ray forms it in float as well (the FP64 azimuth rounded once): a
+    // general double sincos per step would dominate the FP64 step.
     BH_DEV static f3 cart(R rs, float y, R phi)
     {
-        R sp, cp, px, pz;
-        sincos_fast(phi, sp, cp);
-        mul2_p(rs, -rs, cp, sp, px, pz);
-        return v3((float)px, y, (float)pz);
+        float sp, cp, px, pz;
+        sincos_fast((float)phi, sp, cp);
+        mul2_p((float)rs, -(float)rs, cp, sp, px, pz);
+        return v3(px, y, pz);
     }
 
     // The disk chord from the previous point to the current one (reference
@@ -845,7 +856,7 @@ struct KerrRay
 // MIXED polar passage: the ray continues as an FP64 ray (same method, same
 // termination tests and disk chords, E and Lz as the FP32 ray holds them) with
 // its state carried in FP64 from step to step, until it leaves the cap
-// |sin th| < 1/16 or terminates; then the state is rounded back once.  The
+// |sin th| < kPolarCap or terminates; then the state is rounded back once.  The
 // step that decided to enter is taken here, so the call advances at least one
 // step.  Returns true when the ray terminated.  Out of line: the FP32 step
 // loop keeps its register budget.
@@ -871,7 +882,7 @@ __device__ __noinline__ bool KerrRay<R, STATS, MIXED>::polar_passage_fp64(const 
         bool done = false;
         // bounded by the step budget: every iteration takes a step or terminates
         while (!(done = d.advance(P)))
-            if (abs_p(d.s) >= 0.0625) break;
+            if (abs_p(d.s) >= (double)kPolarCap) break;
         r = (R)d.r; th = (R)d.th; ph = (R)d.ph; pr = (R)d.pr; pth = (R)d.pth;
         tFlight = (R)d.tFlight;
         prevPos = d.prevPos; prevCart = true; accum = d.accum; trans = d.trans; maxHviol = d.maxHviol;

@@ -118,6 +118,39 @@ BH_DEV void sincos_fast(float x, float& s, float& c)
 
 // Accurate versions for the double-precision integrator.
 BH_DEV void sincos_polar(double x, double& s, double& c) { sincos(x, &s, &c); }
+
+// sin/cos in double for angles near either pole: the Taylor series to degree
+// 13 (sin) and 12 (cos) for |x| <= 0.2 (remainder below 1e-17 relative), and
+// for |pi - x| <= 0.2 through sin(pi - t) = sin t, cos(pi - t) = -cos t with
+// pi - x formed in two parts; the library sincos elsewhere.  Polar angles of
+// the FP64 steps near the spin axis lie in that range, where this costs a
+// dozen FMAs instead of a general argument reduction.
+BH_DEV void sincos_cap(double x, double& s, double& c)
+{
+    const double PI_HI = 3.141592653589793116, PI_LO = 1.2246467991473532e-16;
+    double t = x, sc = 1.0;
+    if (fabs(x) > 0.2)
+    {
+        if (fabs(PI_HI - x) > 0.2) { sincos(x, &s, &c); return; }
+        t = (PI_HI - x) + PI_LO;
+        sc = -1.0;
+    }
+    const double t2 = t * t;
+    double ps = -1.0 / 6227020800.0;                 // -1/13!
+    ps = fma(ps, t2, 1.0 / 39916800.0);
+    ps = fma(ps, t2, -1.0 / 362880.0);
+    ps = fma(ps, t2, 1.0 / 5040.0);
+    ps = fma(ps, t2, -1.0 / 120.0);
+    ps = fma(ps, t2, 1.0 / 6.0);
+    s = fma(-t * t2, ps, t);                         // t - t^3/3! + t^5/5! - ...
+    double pc = 1.0 / 479001600.0;                   // 1/12!
+    pc = fma(pc, t2, -1.0 / 3628800.0);
+    pc = fma(pc, t2, 1.0 / 40320.0);
+    pc = fma(pc, t2, -1.0 / 720.0);
+    pc = fma(pc, t2, 1.0 / 24.0);
+    pc = fma(pc, t2, -0.5);
+    c = sc * fma(pc, t2, 1.0);                       // 1 - t^2/2! + t^4/4! - ...
+}
 BH_DEV void sincos_fast(double x, double& s, double& c) { sincos(x, &s, &c); }
 
 // precision-generic elementary functions

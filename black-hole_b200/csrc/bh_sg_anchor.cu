@@ -1,0 +1,257 @@
+// ---------------------------------------------------------------------------
+// bh_sg_anchor.cu -- resolve pass of the anchored surrogate frame.
+//
+// An anchored frame traces one pixel in S x S with the FP32 RK4 tracer (the
+// anchors, exact pixels of the plain frame) and builds every other pixel of
+// a smooth sky region from them:
+//   * the escape direction is the Catmull-Rom (bicubic) interpolation of the
+//     4 x 4 surrounding anchors' escape directions; its error is bounded by
+//     twice the distance between the bicubic and the bilinear interpolants
+//     (the bilinear error term dominates the bicubic one wherever the map is
+//     smooth), plus a floor of 2e-6 rad;
+//   * the pixel is accepted only if all 16 anchors escaped without touching
+//     the disk, the optional cell gate (the network's probability that the
+//     cell centre escapes without the disk) passes, the bound is below
+//     epsMax, and the sky is flat within the bound: either no star of the
+//     four star lattices lies within reach of the bound (an exact test on the
+//     lattice cell and the cell's star), or the display values (exposure,
+//     ACES, vibrance, gamma, before dither, in byte units) of the sky at the
+//     direction and at four directions sqrt(2) bound away differ by less
+//     than maxStep; and the pixel stays below the bloom bright-pass
+//     threshold, so neither its byte nor its neighbours' bloom can move by
+//     a whole step;
+//   * everything else goes on the RK4 list.
+// The sky is the reference's backgroundColor (trace.cuh:166-195) at the
+// interpolated direction, times the transmittance 1 of a sky-only ray
+// (renderSampleHDR, trace.cuh:908-926).
+// No counterpart in the reference.
+// ---------------------------------------------------------------------------
+#include "bh_integrate.cuh"
+#include "bh_post.cuh"
+#include "bh_sg_infer.h"
+
+namespace {
+
+constexpr float kLumBloomSafe = 0.9f;     // bright pass starts at 0.95 (post_process.cuh:76-84)
+
+__device__ __forceinline__ void catmull_rom(float t, float w[4])
+{
+    const float t2 = t * t, t3 = t2 * t;
+    w[0] = 0.5f * (-t3 + 2.f * t2 - t);
+    w[1] = 0.5f * (3.f * t3 - 5.f * t2 + 2.f);
+    w[2] = 0.5f * (-3.f * t3 + 4.f * t2 + t);
+    w[3] = 0.5f * (t3 - t2);
+}
+
+// display value of one HDR colour before dither and quantisation, in byte units
+// (finalize_pixel without bloom and dither: exposure, ACES, vibrance, gamma)
+__device__ __forceinline__ f3 display_value(f3 hdr, float exposure)
+{
+    f3 c = aces_x(v3(hdr.x * exposure, hdr.y * exposure, hdr.z * exposure));
+    const float lum = 0.2126f * c.x + 0.7152f * c.y + 0.0722f * c.z;
+    c = v3(clampf(lum + (c.x - lum) * 1.12f, 0.f, 1.f), clampf(lum + (c.y - lum) * 1.12f, 0.f, 1.f),
+           clampf(lum + (c.z - lum) * 1.12f, 0.f, 1.f));
+    const float g = 1.f / 2.2f;
+    return v3(255.f * __powf(c.x, g), 255.f * __powf(c.y, g), 255.f * __powf(c.z, g));
+}
+
+__device__ __forceinline__ float lum_exposed(f3 c, float exposure)
+{
+    return exposure * (0.2126f * c.x + 0.7152f * c.y + 0.0722f * c.z);
+}
+
+// Is one star lattice (trace.cuh:131-164: `cell` cells per unit direction, one
+// candidate star per cell, drawn only inside its own cell and only where
+// d2 * sharp <= cut) free of stars everywhere within `r` of the direction d?
+// True when the whole disc stays inside d's cell (all cell faces farther than
+// the margin) and the cell's star, cut radius included, lies beyond it.  The
+// cell and star position use the same exact operations as star_layer.
+__device__ __forceinline__ bool star_layer_clear(f3 d, float cell, float sharp, float r)
+{
+    const f3 p = v3(mul_x(d.x, cell), mul_x(d.y, cell), mul_x(d.z, cell));
+    const f3 id = v3(floorf(p.x), floorf(p.y), floorf(p.z));
+    const f3 f = v3(sub_x(p.x, id.x), sub_x(p.y, id.y), sub_x(p.z, id.z));
+    const float m = 1.5f * r * cell + 1e-5f;     // the offsets reach sqrt(2) r; margin in cell units
+    const float face = fminf(fminf(fminf(f.x, 1.f - f.x), fminf(f.y, 1.f - f.y)), fminf(f.z, 1.f - f.z));
+    if (face <= m) return false;
+    const f3 h = hash33(id);
+    const f3 dv = v3(f.x - (0.10f + 0.80f * h.x), f.y - (0.10f + 0.80f * h.y), f.z - (0.10f + 0.80f * h.z));
+    const float dist = sqrtf(dot3(dv, dv));
+    const float mag = hash12(add_x(id.x, mul_x(91.7f, id.z)), sub_x(id.y, mul_x(33.1f, id.x)));
+    const float cut = (mag > 0.9f) ? 60.f : 14.f;
+    return dist - m > sqrtf(cut / sharp);
+}
+
+// No star of the four lattices of backgroundColor within r of d: the rest of the
+// sky (Milky-Way band and airglow) varies on scales of 0.1 rad and more.
+__device__ __forceinline__ bool stars_clear(f3 d, float r)
+{
+    return star_layer_clear(d, 80.f, 320.f, r) && star_layer_clear(d, 190.f, 520.f, r) &&
+           star_layer_clear(d, 420.f, 820.f, r) && star_layer_clear(d, 900.f, 1500.f, r);
+}
+
+__device__ __forceinline__ f3 unit3(f3 v)
+{
+    const float l = rsqrtf(fmaxf(v.x * v.x + v.y * v.y + v.z * v.z, 1e-30f));
+    return v3(v.x * l, v.y * l, v.z * l);
+}
+
+__device__ __forceinline__ void push(unsigned* list, unsigned* count, unsigned pix, bool want)
+{
+    const unsigned lane = threadIdx.x & 31u;
+    const unsigned m = __ballot_sync(0xffffffffu, want);
+    if (!m) return;
+    unsigned base = 0;
+    if (lane == (unsigned)(__ffs(m) - 1)) base = atomicAdd(count, (unsigned)__popc(m));
+    base = __shfl_sync(0xffffffffu, base, __ffs(m) - 1);
+    if (want) list[base + __popc(m & ((1u << lane) - 1u))] = pix;
+}
+
+// One thread per pixel; 2-D blocks of 32 x 8 pixels (the warp is one row of 32).
+__global__ void __launch_bounds__(256) anchor_resolve_kernel(const __grid_constant__ SgAnchorFrame F)
+{
+    const TraceParams& P = F.tp;
+    const int x = blockIdx.x * 32 + (threadIdx.x & 31), y = blockIdx.y * 8 + (threadIdx.x >> 5);
+    const bool inFrame = x < P.W && y < P.H;
+    const int S = F.S;
+    const unsigned pix = inFrame ? (unsigned)y * (unsigned)P.W + (unsigned)x : 0u;
+    float4* acc = reinterpret_cast<float4*>(P.out);
+
+    bool anchor = false, resolved = false;
+    f3 hdr = v3(0.f, 0.f, 0.f);
+    int reason = 0;                   // 1 anchors / cell gate, 2 error bound, 3 sky sensitivity
+    if (inFrame)
+    {
+        const int cx = x / S, cy = y / S;
+        if (x == cx * S && y == cy * S)
+        {   // an anchor: its own RK4 sample
+            const BHAnchor& a = F.anchors[cy * F.nx + cx];
+            hdr = v3(a.hdr.x, a.hdr.y, a.hdr.z);
+            anchor = true;
+        }
+        else if (cx >= 1 && cy >= 1 && cx + 2 < F.nx && cy + 2 < F.ny)
+        {
+            bool sky = true;
+            if (F.cellGate) sky = F.cellGate[cy * (F.nx - 1) + cx].x >= F.minProb;
+            f3 d[4][4];
+#pragma unroll
+            for (int j = 0; j < 4; ++j)
+#pragma unroll
+                for (int i = 0; i < 4; ++i)
+                {
+                    const BHAnchor& a = F.anchors[(cy - 1 + j) * F.nx + (cx - 1 + i)];
+                    sky = sky && a.flags == BH_ANCHOR_ESCAPED;
+                    d[j][i] = v3(a.escDir.x, a.escDir.y, a.escDir.z);
+                }
+            reason = 1;
+            if (sky)
+            {
+                const float tx = (float)(x - cx * S) / (float)S, ty = (float)(y - cy * S) / (float)S;
+                float wx[4], wy[4];
+                catmull_rom(tx, wx);
+                catmull_rom(ty, wy);
+                f3 bc = v3(0.f, 0.f, 0.f);
+#pragma unroll
+                for (int j = 0; j < 4; ++j)
+#pragma unroll
+                    for (int i = 0; i < 4; ++i)
+                    {
+                        const float w = wy[j] * wx[i];
+                        bc = v3(bc.x + w * d[j][i].x, bc.y + w * d[j][i].y, bc.z + w * d[j][i].z);
+                    }
+                const f3 top = v3(d[1][1].x + tx * (d[1][2].x - d[1][1].x), d[1][1].y + tx * (d[1][2].y - d[1][1].y),
+                                  d[1][1].z + tx * (d[1][2].z - d[1][1].z));
+                const f3 bot = v3(d[2][1].x + tx * (d[2][2].x - d[2][1].x), d[2][1].y + tx * (d[2][2].y - d[2][1].y),
+                                  d[2][1].z + tx * (d[2][2].z - d[2][1].z));
+                const f3 bl = unit3(v3(top.x + ty * (bot.x - top.x), top.y + ty * (bot.y - top.y),
+                                       top.z + ty * (bot.z - top.z)));
+                bc = unit3(bc);
+                const f3 df = v3(bc.x - bl.x, bc.y - bl.y, bc.z - bl.z);
+                const float eps = 2.f * sqrtf(df.x * df.x + df.y * df.y + df.z * df.z) + 2e-6f;
+                reason = 2;
+                if (eps <= F.epsMax)
+                {
+                    const f3 c0 = sky_color(bc, P.gCam);
+                    const f3 y0 = display_value(c0, P.exposure);
+                    bool flat = lum_exposed(c0, P.exposure) < kLumBloomSafe;
+                    // no star within reach: flat without sampling (the common case)
+                    const bool clear = flat && stars_clear(normalize_x(bc), eps);
+                    // two unit vectors orthogonal to the direction
+                    const f3 ref = fabsf(bc.y) < 0.9f ? v3(0.f, 1.f, 0.f) : v3(1.f, 0.f, 0.f);
+                    const f3 u = unit3(v3(ref.y * bc.z - ref.z * bc.y, ref.z * bc.x - ref.x * bc.z,
+                                          ref.x * bc.y - ref.y * bc.x));
+                    const f3 v = v3(bc.y * u.z - bc.z * u.y, bc.z * u.x - bc.x * u.z, bc.x * u.y - bc.y * u.x);
+                    const float r = 1.41421356f * eps;
+#pragma unroll 1
+                    for (int k = 0; k < 4 && flat && !clear; ++k)
+                    {
+                        const float su = (k == 0) ? r : (k == 1 ? -r : 0.f);
+                        const float sv = (k == 2) ? r : (k == 3 ? -r : 0.f);
+                        const f3 dk = unit3(v3(bc.x + su * u.x + sv * v.x, bc.y + su * u.y + sv * v.y,
+                                               bc.z + su * u.z + sv * v.z));
+                        const f3 ck = sky_color(dk, P.gCam);
+                        const f3 yk = display_value(ck, P.exposure);
+                        flat = lum_exposed(ck, P.exposure) < kLumBloomSafe && fabsf(yk.x - y0.x) < F.maxStep &&
+                               fabsf(yk.y - y0.y) < F.maxStep && fabsf(yk.z - y0.z) < F.maxStep;
+                    }
+                    reason = 3;
+                    if (flat && isfinite(c0.x) && isfinite(c0.y) && isfinite(c0.z))
+                    {
+                        hdr = c0;
+                        resolved = true;
+                        reason = 0;
+                    }
+                }
+            }
+        }
+        else reason = 1;
+    }
+    if (anchor || resolved) acc[pix] = make_float4(hdr.x, hdr.y, hdr.z, 1.f);
+
+    // held-out sample of the interpolated pixels (hashed per frame), also traced and compared
+    bool held = false;
+    if (resolved && F.heldStride > 0)
+    {
+        unsigned h = pix * 0x9E3779B1u ^ (F.frameSeed * 0x85EBCA77u);
+        h ^= h >> 15; h *= 0x2C1B3C6Du; h ^= h >> 12;
+        held = (h % (unsigned)F.heldStride) == 0u;
+    }
+    const bool trace = inFrame && !anchor && !resolved;
+    push(F.list, F.listCount, pix, trace || held);
+    const unsigned lane = threadIdx.x & 31u;
+    const unsigned mh = __ballot_sync(0xffffffffu, held);
+    if (mh)
+    {
+        unsigned base = 0;
+        if (lane == (unsigned)(__ffs(mh) - 1)) base = atomicAdd(F.heldCount, (unsigned)__popc(mh));
+        base = __shfl_sync(0xffffffffu, base, __ffs(mh) - 1);
+        if (held)
+        {
+            const unsigned k = base + __popc(mh & ((1u << lane) - 1u));
+            if (k < F.heldCap)
+            {
+                F.heldPix[k] = pix;
+                F.heldPred[k] = make_float4(hdr.x, hdr.y, hdr.z, 1.f);
+            }
+        }
+    }
+    // per-frame tallies: interpolated pixels and the rejection reason of the others
+#pragma unroll
+    for (int k = 0; k < 4; ++k)
+    {
+        const bool mine = inFrame && !anchor && (k == 0 ? resolved : reason == k);
+        const unsigned m = __ballot_sync(0xffffffffu, mine);
+        if (lane == 0 && m) atomicAdd(F.stats + k, (unsigned)__popc(m));
+    }
+}
+
+}  // namespace
+
+cudaError_t sg_anchor_resolve(const SgAnchorFrame& F, cudaStream_t s)
+{
+    const TraceParams& P = F.tp;
+    if (F.S < 2 || F.nx < 1 || F.ny < 1) return cudaErrorInvalidValue;
+    dim3 grid((P.W + 31) / 32, (P.H + 7) / 8);
+    anchor_resolve_kernel<<<grid, 256, 0, s>>>(F);
+    return cudaGetLastError();
+}

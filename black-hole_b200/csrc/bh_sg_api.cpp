@@ -121,6 +121,17 @@ struct BHSurrogate
     float* bIn = nullptr;
     float* bTgt = nullptr;
     int bCap = 0;
+    // anchored frames: RK4 anchors every anchorStride pixels (0: the network's own directions)
+    int anchorStride = 4;
+    bool anchorNet = true;
+    float epsMax = 1e-4f, maxStep = 0.5f;
+    int aW = 0, aH = 0, aS = 0, aNx = 0, aNy = 0;
+    unsigned* anchorPix = nullptr;    // anchor pixels, row-major
+    BHAnchor* anchorRec = nullptr;
+    unsigned* cellPix = nullptr;      // cell-centre pixels
+    float2* cellGate = nullptr;
+    size_t aCap = 0, cCap = 0;
+    unsigned lastAnchors = 0;
 };
 
 namespace {
@@ -130,7 +141,8 @@ void freeAll(BHSurrogate* s)
     SgState& S = s->S;
     sg_free_batch(S);
     void* ps[] = {S.params, S.grads, S.adamM, S.adamV, S.W, S.Wt, S.biasPacked, S.loss, S.dsIn, S.dsTgt, s->list,
-                  s->counters, s->heldPix, s->heldPred, s->bIn, s->bTgt};
+                  s->counters, s->heldPix, s->heldPred, s->bIn, s->bTgt, s->anchorPix, s->anchorRec, s->cellPix,
+                  s->cellGate};
     for (void* p : ps)
         if (p) cudaFree(p);
     if (s->stream) cudaStreamDestroy(s->stream);
@@ -213,6 +225,110 @@ cudaError_t ensureFrame(BHSurrogate* s, size_t pixels)
     s->listCap = pixels;
     s->heldCap = cap;
     return cudaSuccess;
+}
+
+// Anchor lattice of a W x H frame: pixels (S ax, S ay), and the centres of the
+// (nx - 1) x (ny - 1) cells between them; built once per size and stride
+// (blocking upload).
+cudaError_t ensureAnchors(BHSurrogate* s, int W, int H, int S)
+{
+    if (s->aW == W && s->aH == H && s->aS == S && s->anchorPix) return cudaSuccess;
+    const int nx = (W - 1) / S + 1, ny = (H - 1) / S + 1;
+    const size_t nA = (size_t)nx * ny, nC = (size_t)std::max(nx - 1, 1) * std::max(ny - 1, 1);
+    cudaError_t e = cudaSuccess;
+    if (nA > s->aCap)
+    {
+        if (s->anchorPix) cudaFree(s->anchorPix);
+        if (s->anchorRec) cudaFree(s->anchorRec);
+        s->anchorPix = nullptr; s->anchorRec = nullptr; s->aCap = 0;
+        if ((e = bh_device_alloc(reinterpret_cast<void**>(&s->anchorPix), nA * sizeof(unsigned)))) return e;
+        if ((e = bh_device_alloc(reinterpret_cast<void**>(&s->anchorRec), nA * sizeof(BHAnchor)))) return e;
+        s->aCap = nA;
+    }
+    if (nC > s->cCap)
+    {
+        if (s->cellPix) cudaFree(s->cellPix);
+        if (s->cellGate) cudaFree(s->cellGate);
+        s->cellPix = nullptr; s->cellGate = nullptr; s->cCap = 0;
+        if ((e = bh_device_alloc(reinterpret_cast<void**>(&s->cellPix), nC * sizeof(unsigned)))) return e;
+        if ((e = bh_device_alloc(reinterpret_cast<void**>(&s->cellGate), nC * sizeof(float2)))) return e;
+        s->cCap = nC;
+    }
+    std::vector<unsigned> a(nA), c(nC, 0u);
+    for (int y = 0; y < ny; ++y)
+        for (int x = 0; x < nx; ++x) a[(size_t)y * nx + x] = (unsigned)(y * S) * (unsigned)W + (unsigned)(x * S);
+    for (int y = 0; y + 1 < ny; ++y)
+        for (int x = 0; x + 1 < nx; ++x)
+            c[(size_t)y * (nx - 1) + x] = (unsigned)(y * S + S / 2) * (unsigned)W + (unsigned)(x * S + S / 2);
+    if ((e = cudaMemcpy(s->anchorPix, a.data(), nA * sizeof(unsigned), cudaMemcpyHostToDevice))) return e;
+    if ((e = cudaMemcpy(s->cellPix, c.data(), nC * sizeof(unsigned), cudaMemcpyHostToDevice))) return e;
+    s->aW = W; s->aH = H; s->aS = S; s->aNx = nx; s->aNy = ny;
+    return cudaSuccess;
+}
+
+// The anchored frame: cell gate (network), RK4 anchors, resolve pass; the RK4
+// list, held-out comparison and post-processing follow in bhSurrogateRender.
+cudaError_t anchoredFrame(BHSurrogate* s, const RenderParams& P, float4* accum, cudaStream_t stream)
+{
+    const int S = s->anchorStride;
+    cudaError_t e = ensureAnchors(s, P.width, P.height, S);
+    if (e != cudaSuccess) return e;
+    const unsigned nA = (unsigned)(s->aNx * s->aNy);
+    const unsigned nC = (unsigned)((s->aNx - 1) * (s->aNy - 1));
+    if (s->anchorNet && s->aNx > 1 && s->aNy > 1)
+    {
+        SgState& S_ = s->S;
+        SgFrame F{};
+        F.tp = bh_frame_params(P, BH_OUT_ACCUM, accum);
+        sceneInputs(P, F.aN, F.qN, F.rN, F.iN);
+        F.evalPix = s->cellPix;
+        F.gateOut = s->cellGate;
+        SgInferArgs a{S_.W, S_.W + 4 * kHidW, S_.biasPacked, nullptr, nullptr, nC, S_.err};
+        if ((e = sg_infer_launch(a, &F, stream)) != cudaSuccess) return e;
+    }
+    TraceParams t = bh_frame_params(P, BH_OUT_ANCHOR, s->anchorRec);
+    t.pixList = s->anchorPix;
+    t.nRays = nA;
+    if ((e = bh_device_counter(&t.counter)) != cudaSuccess) return e;
+    if ((e = bh_launch_trace(t, BH_PREC_FP32, false, bh_family_blocks(P), stream)) != cudaSuccess) return e;
+    SgAnchorFrame A{};
+    A.tp = bh_frame_params(P, BH_OUT_ACCUM, accum);
+    A.anchors = s->anchorRec;
+    A.S = S; A.nx = s->aNx; A.ny = s->aNy;
+    A.cellGate = s->anchorNet ? s->cellGate : nullptr;
+    A.minProb = s->minProb;
+    A.epsMax = s->epsMax;
+    A.maxStep = s->maxStep;
+    A.list = s->list;
+    A.listCount = s->counters;
+    A.heldPix = s->heldPix;
+    A.heldPred = s->heldPred;
+    A.heldCount = s->counters + 1;
+    A.heldCap = s->heldCap;
+    A.heldStride = s->heldStride;
+    A.frameSeed = ++s->frames;
+    A.stats = s->counters + 8;
+    s->lastAnchors = nA;
+    return sg_anchor_resolve(A, stream);
+}
+
+// RK4 for the listed pixels (the tracer reads the list and its device-side
+// length), the held-out comparison, then bloom and tonemap.
+cudaError_t traceListAndPost(BHSurrogate* s, const RenderParams& P, uchar4* out, float4* accum, float4* bloomA,
+                             float4* bloomB, cudaStream_t stream)
+{
+    TraceParams t = bh_frame_params(P, BH_OUT_ACCUM, accum);
+    t.pixList = s->list;
+    t.nRaysDev = s->counters;
+    t.nRays = (unsigned)((size_t)P.width * P.height);
+    cudaError_t e = bh_device_counter(&t.counter);
+    if (e != cudaSuccess) return e;
+    if ((e = bh_launch_trace(t, BH_PREC_FP32, false, bh_family_blocks(P), stream)) != cudaSuccess) return e;
+    if ((e = sg_held_compare(accum, s->heldPix, s->heldPred, s->counters + 1, s->heldCap, t, s->counters + 4,
+                             stream)) != cudaSuccess)
+        return e;
+    PostConsts pc{P.exposure, P.bloomStrength, P.bloomEnabled ? 1 : 0, P.swapRB};
+    return bh_launch_post(out, accum, bloomB, bloomA, P.width, P.height, pc, stream);
 }
 
 }  // namespace
@@ -448,6 +564,14 @@ cudaError_t bhSurrogateRender(BHSurrogate* s, uchar4* out, float4* accum, float4
     const size_t pixels = (size_t)P.width * P.height;
     cudaError_t e = ensureFrame(s, pixels);
     if (e != cudaSuccess) return e;
+    s->lastPixels = (unsigned)pixels;
+    if (s->anchorStride >= 2)
+    {
+        if ((e = cudaMemsetAsync(s->counters, 0, 64, stream)) != cudaSuccess) return e;
+        if ((e = anchoredFrame(s, P, accum, stream)) != cudaSuccess) return e;
+        return traceListAndPost(s, P, out, accum, bloomA, bloomB, stream);
+    }
+    s->lastAnchors = 0;
     CritKey key;
     key.model = P.model; key.maxSteps = P.maxSteps; key.M = P.M; key.a = P.aSpin; key.Q = P.Qc;
     key.dist = length3(P.camPos); key.cosIncl = P.camPos.y / key.dist; key.tanHalfFov = P.tanHalfFov;
@@ -474,22 +598,10 @@ cudaError_t bhSurrogateRender(BHSurrogate* s, uchar4* out, float4* accum, float4
     F.heldCap = s->heldCap;
     F.heldStride = s->heldStride;
     F.frameSeed = ++s->frames;
-    s->lastPixels = (unsigned)pixels;
     if ((e = cudaMemsetAsync(s->counters, 0, 64, stream)) != cudaSuccess) return e;
     SgInferArgs a{S.W, S.W + 4 * kHidW, S.biasPacked, nullptr, nullptr, (unsigned)pixels, S.err};
     if ((e = sg_infer_launch(a, &F, stream)) != cudaSuccess) return e;
-    // RK4 for the listed pixels
-    TraceParams t = F.tp;
-    t.pixList = s->list;
-    t.nRaysDev = s->counters;
-    t.nRays = (unsigned)pixels;
-    if ((e = bh_device_counter(&t.counter)) != cudaSuccess) return e;
-    if ((e = bh_launch_trace(t, BH_PREC_FP32, false, bh_family_blocks(P), stream)) != cudaSuccess) return e;
-    if ((e = sg_held_compare(accum, s->heldPix, s->heldPred, s->counters + 1, s->heldCap, F.tp, s->counters + 4,
-                             stream)) != cudaSuccess)
-        return e;
-    PostConsts pc{P.exposure, P.bloomStrength, P.bloomEnabled ? 1 : 0, P.swapRB};
-    return bh_launch_post(out, accum, bloomB, bloomA, P.width, P.height, pc, stream);
+    return traceListAndPost(s, P, out, accum, bloomA, bloomB, stream);
 }
 
 cudaError_t bhSurrogateFrameStats(BHSurrogate* s, BHSurrogateStats* st)
@@ -508,6 +620,12 @@ cudaError_t bhSurrogateFrameStats(BHSurrogate* s, BHSurrogateStats* st)
     std::memcpy(&mx, &c[6], sizeof(float));
     st->heldOutMaxAbs = mx;
     st->heldOutOverTol = c[7];
+    st->anchors = s->lastAnchors;
+    st->rk4Pixels += s->lastAnchors;
+    st->interpolated = c[8];
+    st->rejectAnchors = c[9];
+    st->rejectBound = c[10];
+    st->rejectSky = c[11];
     return cudaSuccess;
 }
 
@@ -522,6 +640,18 @@ extern "C" cudaError_t bhSurrogateDatasetCopy(BHSurrogate* s, float* in, float* 
     if (e == cudaSuccess && tgt)
         e = cudaMemcpy(tgt, s->S.dsTgt + first * 8, (size_t)count * 8 * sizeof(float), cudaMemcpyDeviceToHost);
     return e;
+}
+
+extern "C" cudaError_t bhSurrogateSetAnchors(BHSurrogate* s, int stride, int useNetwork, float epsMax,
+                                             float maxStep)
+{
+    if (!s || stride < 0 || stride == 1 || stride > 64 || !(epsMax > 0.f) || !(maxStep > 0.f && maxStep <= 1.f))
+        return cudaErrorInvalidValue;
+    s->anchorStride = stride;
+    s->anchorNet = useNetwork != 0;
+    s->epsMax = epsMax;
+    s->maxStep = maxStep;
+    return cudaSuccess;
 }
 
 extern "C" cudaError_t bhSurrogateSetGate(BHSurrogate* s, float minProb, float minConf, float critBand, int heldStride)

@@ -290,7 +290,8 @@ sg_infer_kernel(const __grid_constant__ CUtensorMap tW, const __grid_constant__ 
             RayIn r;
             if constexpr (FRAME)
             {
-                frame_inputs(F, valid ? rid : 0u, r);
+                const unsigned pix = valid ? (F.evalPix ? __ldg(F.evalPix + rid) : rid) : 0u;
+                frame_inputs(F, pix, r);
             }
             else
             {
@@ -347,7 +348,16 @@ sg_infer_kernel(const __grid_constant__ CUtensorMap tW, const __grid_constant__ 
                 for (int k = 0; k < kOut; ++k) y[k] += sBias[kHidden * kWidth + k];
                 if constexpr (FRAME)
                 {
-                    frame_output(F, rid, valid, r, y);
+                    if (F.gateOut)
+                    {   // cell gate of an anchored frame: P(escaped without the disk), confidence
+                        if (valid)
+                        {
+                            const float m = fmaxf(y[0], fmaxf(y[1], y[2]));
+                            const float e0 = __expf(y[0] - m), e1 = __expf(y[1] - m), e2 = __expf(y[2] - m);
+                            F.gateOut[rid] = make_float2(e0 / (e0 + e1 + e2), 1.f / (1.f + __expf(-y[kOConf])));
+                        }
+                    }
+                    else frame_output(F, rid, valid, r, y);
                 }
                 else if (valid)
                 {

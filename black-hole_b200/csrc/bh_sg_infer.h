@@ -28,6 +28,10 @@ struct SgFrame
     unsigned heldCap;
     int heldStride;                 // 1 in heldStride surrogate pixels is held out (0: none)
     unsigned frameSeed;
+    // cell-gate mode (anchored frames): ray k is pixel evalPix[k]; instead of deciding the
+    // pixel, the kernel writes (probability of "escaped without the disk", confidence) to gateOut[k]
+    const unsigned* evalPix;
+    float2* gateOut;
 };
 
 struct SgInferArgs
@@ -43,6 +47,34 @@ struct SgInferArgs
 
 // frame == nullptr: raw mode (rawIn -> rawOut)
 cudaError_t sg_infer_launch(const SgInferArgs& a, const SgFrame* frame, cudaStream_t s);
+
+// Anchored surrogate frame (bh_sg_anchor.cu).  The anchors are the pixels
+// (S ax, S ay), ax < nx = (W - 1) / S + 1, ay < ny = (H - 1) / S + 1, traced
+// by RK4 into `anchors` (row-major, BH_OUT_ANCHOR records).  The resolve pass
+// writes every anchor's HDR and every pixel it can interpolate to the
+// accumulation buffer (tp.out) and appends the rest to `list`.
+struct SgAnchorFrame
+{
+    TraceParams tp;
+    const BHAnchor* anchors;
+    int S, nx, ny;
+    const float2* cellGate;         // null, or per cell (nx - 1) x (ny - 1): (P(sky), confidence)
+    float minProb;                  // cell gate: P(escaped without the disk) needed at the cell centre
+    float epsMax;                   // largest interpolation error bound (rad) a pixel may have
+    float maxStep;                  // sensitivity bar: display-value change (byte units) within the bound
+    unsigned* list;
+    unsigned* listCount;
+    unsigned* heldPix;
+    float4* heldPred;
+    unsigned* heldCount;
+    unsigned heldCap;
+    int heldStride;
+    unsigned frameSeed;
+    unsigned* stats;                // [0] interpolated, [1] rejected by the anchors / cell gate,
+                                    // [2] by the error bound, [3] by the sky sensitivity
+};
+
+cudaError_t sg_anchor_resolve(const SgAnchorFrame& F, cudaStream_t s);
 
 // Held-out comparison after the RK4 pass: stats[0] += pixels compared,
 // stats[1] += pixels whose RGBA8 (exposure, no bloom) differs by more than

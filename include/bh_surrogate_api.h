@@ -116,14 +116,23 @@ cudaError_t bhSurrogateTrain(BHSurrogate* s, int steps, int batch, float lr, uns
 
 /* Render one frame with the surrogate: same buffers and result layout as
  * launchRenderPipeline.  Requires an orbit camera (looking at the hole, no
- * roll: camRight.y == 0) and accumMode 0.  The fused kernel resolves the
- * pixels it is sure of (escaped or captured without the disk, class
- * probability and confidence >= 0.95, farther than 2 % from the critical
- * curve); the rest, plus a held-out sample of 1 in 256 of the resolved
- * pixels, go through the FP32 RK4 tracer; then bloom and tonemap.  The
- * critical curve (per polar angle on the screen) is found by RK4 bisection
- * once per metric, camera distance, inclination and field of view, and
- * cached (that first call blocks). */
+ * roll: camRight.y == 0) and accumMode 0.  Two forms (bhSurrogateSetAnchors):
+ *  - anchored (the default, anchor stride 4): the FP32 RK4 tracer traces one
+ *    pixel in stride x stride (the anchors); a pixel between anchors takes the
+ *    bicubic interpolation of the 4 x 4 surrounding anchors' escape directions
+ *    when all 16 escaped without touching the disk, the network gives its cell
+ *    centre a probability >= minProb of escaping without the disk, the
+ *    interpolation error bound is <= epsMax and the sky is flat within that
+ *    bound (display values within maxStep of a byte step, below the bloom
+ *    threshold); every other pixel is traced;
+ *  - network (stride 0): the fused kernel resolves the pixels it is sure of
+ *    from its own escape direction (escaped or captured without the disk,
+ *    class probability and confidence >= 0.95, farther than 2 % from the
+ *    critical curve, which is found by RK4 bisection once per metric, camera
+ *    distance, inclination and field of view and cached -- that first call
+ *    blocks); the rest go through the RK4 tracer.
+ * In both forms a held-out sample of 1 in 256 of the resolved pixels is also
+ * traced and compared, then bloom and tonemap run. */
 cudaError_t bhSurrogateRender(BHSurrogate* s, uchar4* out, float4* accum, float4* bloomA, float4* bloomB,
                               const RenderParams* p, cudaStream_t stream);
 
@@ -135,6 +144,13 @@ cudaError_t bhSurrogateRender(BHSurrogate* s, uchar4* out, float4* accum, float4
  * accuracy for speed; heldStride 1 compares every resolved pixel. */
 cudaError_t bhSurrogateSetGate(BHSurrogate* s, float minProb, float minConf, float critBand, int heldStride);
 
+/* Form of bhSurrogateRender (defaults 4, 1, 1e-4, 0.5): anchor stride (0:
+ * the network form; else 2..64), whether the network's cell gate applies,
+ * the largest escape-direction error bound (rad) an interpolated pixel may
+ * have, and the largest display-value change (in byte steps) allowed within
+ * that bound. */
+cudaError_t bhSurrogateSetAnchors(BHSurrogate* s, int stride, int useNetwork, float epsMax, float maxStep);
+
 /* Statistics of the last rendered frame (blocking). */
 typedef struct BHSurrogateStats
 {
@@ -144,6 +160,11 @@ typedef struct BHSurrogateStats
     unsigned heldOutOver1Lsb; /* held-out pixels whose RGBA8 differs by > 1 LSB */
     unsigned heldOutOverTol;  /* held-out pixels with HDR error > 1e-3 relative */
     float heldOutMaxAbs;      /* largest HDR difference on the held-out sample */
+    unsigned anchors;         /* anchored form: anchor pixels (counted in rk4Pixels) */
+    unsigned interpolated;    /* anchored form: pixels built from the anchors */
+    unsigned rejectAnchors;   /* traced: an anchor not sky-only, or the cell gate, or the frame border */
+    unsigned rejectBound;     /* traced: interpolation error bound above epsMax */
+    unsigned rejectSky;       /* traced: sky not flat within the bound */
 } BHSurrogateStats;
 cudaError_t bhSurrogateFrameStats(BHSurrogate* s, BHSurrogateStats* stats);
 
