@@ -470,8 +470,9 @@ def surrogate_leg():
         torch.cuda.synchronize()
         t_first = time.perf_counter() - t0
         # (anchor stride, network cell gate, minProb, minConf, critBand, held-out stride)
-        gates = {"anchored_strict": (4, 1, 0.95, 0.95, 0.02, 256),
-                 "anchored_no_network": (4, 0, 0.95, 0.95, 0.02, 256),
+        gates = {"anchored_strict": (8, 1, 0.95, 0.95, 0.02, 256),
+                 "anchored_no_network": (8, 0, 0.95, 0.95, 0.02, 256),
+                 "anchored_stride4": (4, 1, 0.95, 0.95, 0.02, 256),
                  "network_strict": (0, 1, 0.95, 0.95, 0.02, 256),
                  "network_permissive": (0, 1, 0.5, 0.0, 0.02, 256)}
         res = {}

@@ -601,7 +601,7 @@ struct KerrRay
     // the last step the budget allows: it is needed only if that budget runs out
     BH_DEV static R* last_deriv()
     {
-        __shared__ R dl[BH_TRACE_BLOCK][3];
+        __shared__ R dl[BH_TRACE_BLOCK_MAX][3];
         return dl[threadIdx.x];
     }
 

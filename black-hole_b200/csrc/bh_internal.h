@@ -7,8 +7,13 @@
 #include <vector_types.h>
 #include "bh_trace_params.h"
 
+// Tracing CTAs: 128 threads, except the FP32 Kerr-family render kernels (160
+// threads, 5 CTAs of 80 registers = 25 warps per SM, where 128-thread CTAs fit
+// only 6 x 4 = 24); BH_TRACE_BLOCK_MAX sizes per-thread shared arrays.
 #define BH_TRACE_BLOCK 128
-// resident CTAs per SM the tracing kernels are register-budgeted for
+#define BH_TRACE_BLOCK_KERR 160
+#define BH_TRACE_BLOCK_MAX 160
+// resident CTAs per SM the spherical FP32 tracing kernels are register-budgeted for
 // (65536 / (128 * 7) -> 72 registers per thread, 28 warps per SM)
 #ifndef BH_TRACE_MIN_BLOCKS
 #define BH_TRACE_MIN_BLOCKS 7

@@ -107,15 +107,36 @@ __device__ __forceinline__ void push(unsigned* list, unsigned* count, unsigned p
     if (want) list[base + __popc(m & ((1u << lane) - 1u))] = pix;
 }
 
+// anchors a 32 x 8 pixel block can reach: columns x0/S - 1 .. (x0+31)/S + 2, rows
+// y0/S - 1 .. (y0+7)/S + 2 (at most 19 x 8 for S >= 2)
+constexpr int kAncCols = 19, kAncRows = 8;
+
 // One thread per pixel; 2-D blocks of 32 x 8 pixels (the warp is one row of 32).
+// The block's anchors (escape direction and flags) are staged in shared memory
+// once; each pixel then reads its 4 x 4 neighbourhood from there.
 __global__ void __launch_bounds__(256) anchor_resolve_kernel(const __grid_constant__ SgAnchorFrame F)
 {
+    __shared__ float4 sAnc[kAncRows][kAncCols];
     const TraceParams& P = F.tp;
     const int x = blockIdx.x * 32 + (threadIdx.x & 31), y = blockIdx.y * 8 + (threadIdx.x >> 5);
     const bool inFrame = x < P.W && y < P.H;
     const int S = F.S;
     const unsigned pix = inFrame ? (unsigned)y * (unsigned)P.W + (unsigned)x : 0u;
     float4* acc = reinterpret_cast<float4*>(P.out);
+    const int ax0 = (int)(blockIdx.x * 32) / S - 1, ay0 = (int)(blockIdx.y * 8) / S - 1;
+    for (int i = threadIdx.x; i < kAncRows * kAncCols; i += blockDim.x)
+    {
+        const int r = i / kAncCols, c = i - r * kAncCols;
+        const int ax = ax0 + c, ay = ay0 + r;
+        float4 v = make_float4(0.f, 0.f, 0.f, 0.f);
+        if (ax >= 0 && ay >= 0 && ax < F.nx && ay < F.ny)
+        {
+            const BHAnchor& a = F.anchors[ay * F.nx + ax];
+            v = make_float4(a.escDir.x, a.escDir.y, a.escDir.z, __uint_as_float(a.flags));
+        }
+        sAnc[r][c] = v;
+    }
+    __syncthreads();
 
     bool anchor = false, resolved = false;
     f3 hdr = v3(0.f, 0.f, 0.f);
@@ -138,10 +159,10 @@ __global__ void __launch_bounds__(256) anchor_resolve_kernel(const __grid_consta
             for (int j = 0; j < 4; ++j)
 #pragma unroll
                 for (int i = 0; i < 4; ++i)
-                {
-                    const BHAnchor& a = F.anchors[(cy - 1 + j) * F.nx + (cx - 1 + i)];
-                    sky = sky && a.flags == BH_ANCHOR_ESCAPED;
-                    d[j][i] = v3(a.escDir.x, a.escDir.y, a.escDir.z);
+                {   // anchor (cx - 1 + i, cy - 1 + j), staged at (cy - 1 + j - ay0, cx - 1 + i - ax0)
+                    const float4 a = sAnc[cy - 1 + j - ay0][cx - 1 + i - ax0];
+                    sky = sky && __float_as_uint(a.w) == BH_ANCHOR_ESCAPED;
+                    d[j][i] = v3(a.x, a.y, a.z);
                 }
             reason = 1;
             if (sky)

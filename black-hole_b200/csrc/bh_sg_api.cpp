@@ -122,7 +122,7 @@ struct BHSurrogate
     float* bTgt = nullptr;
     int bCap = 0;
     // anchored frames: RK4 anchors every anchorStride pixels (0: the network's own directions)
-    int anchorStride = 4;
+    int anchorStride = 8;
     bool anchorNet = true;
     float epsMax = 1e-4f, maxStep = 0.5f;
     int aW = 0, aH = 0, aS = 0, aNx = 0, aNy = 0;

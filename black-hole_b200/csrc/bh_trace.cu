@@ -29,13 +29,12 @@
 
 namespace {
 
-constexpr int kWarps = BH_TRACE_BLOCK / 32;
 constexpr int kQueue = 64;            // ring entries per warp (>= 2 x 32)
 constexpr unsigned kChunk = 32;       // ray ids claimed per atomicAdd (one tile)
 
-template <class R, bool STATS> struct Queue;
-template <class R> struct Queue<R, false> { PackedRay<R> s[kWarps][kQueue]; };
-template <class R> struct Queue<R, true> { PackedRay<R> s[kWarps][kQueue]; PackedStats t[kWarps][kQueue]; };
+template <class R, bool STATS, int NW> struct Queue;
+template <class R, int NW> struct Queue<R, false, NW> { PackedRay<R> s[NW][kQueue]; };
+template <class R, int NW> struct Queue<R, true, NW> { PackedRay<R> s[NW][kQueue]; PackedStats t[NW][kQueue]; };
 
 // ray id -> pixel (8x4 tiles, row-major tile order); false when outside the frame
 BH_DEV bool ray_pixel(const TraceParams& P, unsigned rid, int& px, int& py)
@@ -144,23 +143,32 @@ BH_DEV void shade_slot(const TraceParams& P, const PackedRay<typename Ray::Real>
     }
 }
 
-// Register budget (CTAs of 128 threads resident per SM): the spherical FP32
-// render kernel fits 72 registers (7 CTAs); the Kerr-Newman FP32 kernels need
-// 80 (6 CTAs) to stay spill-free in the step loop; FP64 and statistics (probe)
-// kernels carry more state (4 CTAs).  The runtime may run fewer (bhSetTuning).
+// Block size and register budget (CTAs resident per SM): the spherical FP32
+// render kernel fits 72 registers (7 CTAs of 128 threads, 28 warps); the
+// Kerr-Newman FP32 kernels need 80 to stay spill-free in the step loop, which
+// leaves room for 25 warps: 5 CTAs of 160 threads (6 CTAs of 128 threads hold
+// 24; measured 2 % slower on the 4K orbit frames); FP64 and statistics (probe)
+// kernels carry more state (4 CTAs of 128).  The runtime may run fewer
+// (bhSetTuning).
 template <class Ray, bool STATS>
-constexpr int min_blocks()
+__host__ __device__ constexpr int block_of()
 {
-    if (sizeof(typename Ray::Real) != 4 || STATS) return 4;
-    return Ray::kKerrFamily ? 6 : BH_TRACE_MIN_BLOCKS;
+    return (Ray::kKerrFamily && sizeof(typename Ray::Real) == 4 && !STATS) ? BH_TRACE_BLOCK_KERR : BH_TRACE_BLOCK;
 }
 
 template <class Ray, bool STATS>
-__global__ void __launch_bounds__(BH_TRACE_BLOCK, min_blocks<Ray, STATS>())
+__host__ __device__ constexpr int min_blocks()
+{
+    if (sizeof(typename Ray::Real) != 4 || STATS) return 4;
+    return Ray::kKerrFamily ? 5 : BH_TRACE_MIN_BLOCKS;
+}
+
+template <class Ray, bool STATS>
+__global__ void __launch_bounds__(block_of<Ray, STATS>(), min_blocks<Ray, STATS>())
 trace_kernel(const __grid_constant__ TraceParams P)
 {
     using R = typename Ray::Real;
-    __shared__ Queue<R, STATS> Q;
+    __shared__ Queue<R, STATS, block_of<Ray, STATS>() / 32> Q;
     const unsigned lane = threadIdx.x & 31u, warp = threadIdx.x >> 5;
     const unsigned FULL = 0xffffffffu, below = (1u << lane) - 1u;
     PackedRay<R>* ring = Q.s[warp];
@@ -303,7 +311,7 @@ BH_DEV void trace_tile(const TraceParams& P, unsigned tile, unsigned lane, unsig
 // ring.  Plain frames and the surrogate's RK4 pixel lists share this kernel,
 // so a pixel traced by either gets the same bits.
 template <class Ray>
-__global__ void __launch_bounds__(BH_TRACE_BLOCK, min_blocks<Ray, false>())
+__global__ void __launch_bounds__(block_of<Ray, false>(), min_blocks<Ray, false>())
 tile_kernel(const __grid_constant__ TraceParams P)
 {
     const unsigned lane = threadIdx.x & 31u;
@@ -325,11 +333,11 @@ tile_kernel(const __grid_constant__ TraceParams P)
 // frame constants into shared memory when the view changes.  One kernel per
 // metric family, so each runs with its family's register budget.
 template <class Ray>
-__global__ void __launch_bounds__(BH_TRACE_BLOCK, min_blocks<Ray, false>())
+__global__ void __launch_bounds__(block_of<Ray, false>(), min_blocks<Ray, false>())
 batch_kernel(const TraceParams* __restrict__ views, const unsigned* __restrict__ tileBase, int n,
              unsigned totalTiles, unsigned* counter)
 {
-    __shared__ TraceParams sp[kWarps];
+    __shared__ TraceParams sp[block_of<Ray, false>() / 32];
     const unsigned lane = threadIdx.x & 31u, warp = threadIdx.x >> 5;
     const unsigned FULL = 0xffffffffu;
     int cur = -1;
@@ -372,15 +380,16 @@ cudaError_t launch_one(const TraceParams& P, int blocksPerSm, cudaStream_t strea
     if (e != cudaSuccess) return e;
     e = cudaDeviceGetAttribute(&sms, cudaDevAttrMultiProcessorCount, dev);
     if (e != cudaSuccess) return e;
-    e = cudaOccupancyMaxActiveBlocksPerMultiprocessor(&occ, k, BH_TRACE_BLOCK, 0);
+    constexpr int block = block_of<Ray, STATS>();
+    e = cudaOccupancyMaxActiveBlocksPerMultiprocessor(&occ, k, block, 0);
     if (e != cudaSuccess) return e;
     if (occ < 1) occ = 1;
     int per = (blocksPerSm > 0 && blocksPerSm < occ) ? blocksPerSm : occ;
-    long long need = ((long long)P.nRays + BH_TRACE_BLOCK - 1) / BH_TRACE_BLOCK;
+    long long need = ((long long)P.nRays + block - 1) / block;
     long long grid = (long long)per * sms;
     if (grid > need) grid = need;
     if (grid < 1) grid = 1;
-    k<<<(unsigned)grid, BH_TRACE_BLOCK, 0, stream>>>(P);
+    k<<<(unsigned)grid, block, 0, stream>>>(P);
     return cudaGetLastError();
 }
 
@@ -423,20 +432,23 @@ cudaError_t bh_launch_batch(bool kerr, const TraceParams* views, const unsigned*
     int dev = 0, sms = 0, occ = 0;
     if ((e = cudaGetDevice(&dev)) != cudaSuccess) return e;
     if ((e = cudaDeviceGetAttribute(&sms, cudaDevAttrMultiProcessorCount, dev)) != cudaSuccess) return e;
-    if ((e = cudaOccupancyMaxActiveBlocksPerMultiprocessor(&occ, k, BH_TRACE_BLOCK, 0)) != cudaSuccess) return e;
+    const int block = kerr ? block_of<KerrRay<float, false>, false>() : block_of<SphRay<float, false>, false>();
+    if ((e = cudaOccupancyMaxActiveBlocksPerMultiprocessor(&occ, k, block, 0)) != cudaSuccess) return e;
     if (occ < 1) occ = 1;
     const int per = (blocksPerSm > 0 && blocksPerSm < occ) ? blocksPerSm : occ;
     long long grid = (long long)per * sms;
-    const long long need = ((long long)totalTiles * 32 + BH_TRACE_BLOCK - 1) / BH_TRACE_BLOCK;
+    const long long need = ((long long)totalTiles * 32 + block - 1) / block;
     if (grid > need) grid = need;
-    k<<<(unsigned)grid, BH_TRACE_BLOCK, 0, stream>>>(views, tileBase, n, totalTiles, counter);
+    k<<<(unsigned)grid, block, 0, stream>>>(views, tileBase, n, totalTiles, counter);
     return cudaGetLastError();
 }
 
 cudaError_t bh_trace_max_blocks(int model, int* out)
 {
     const bool kerr = (model == 2 || model == 3);
-    return cudaOccupancyMaxActiveBlocksPerMultiprocessor(
-        out, kerr ? trace_kernel<KerrRay<float, false>, false> : trace_kernel<SphRay<float, false>, false>,
-        BH_TRACE_BLOCK, 0);
+    if (kerr)
+        return cudaOccupancyMaxActiveBlocksPerMultiprocessor(out, trace_kernel<KerrRay<float, false>, false>,
+                                                             block_of<KerrRay<float, false>, false>(), 0);
+    return cudaOccupancyMaxActiveBlocksPerMultiprocessor(out, trace_kernel<SphRay<float, false>, false>,
+                                                         block_of<SphRay<float, false>, false>(), 0);
 }

@@ -161,7 +161,8 @@ cudaError_t bhPostProcess(uchar4* out, const float4* accum, float4* bloomA, floa
 
 /* Work-distribution tuning of a metric family (0: Schwarzschild / RN,
  * 1: Kerr / Kerr-Newman): a warp refills its idle lanes once at least
- * `refillMin` (1..32) are idle; `blocksPerSm` CTAs of 128 threads stay
+ * `refillMin` (1..32) are idle; `blocksPerSm` CTAs (160 threads for the
+ * rotating family, 128 for the spherical one) stay
  * resident per SM (0: as many as occupancy allows).  With refillMin = 32 (the
  * default) FP32 renders run the tile-synchronous kernel (a warp traces one
  * 8x4 tile to its last ray, then takes the next); below 32 they run the

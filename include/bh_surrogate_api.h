@@ -117,7 +117,7 @@ cudaError_t bhSurrogateTrain(BHSurrogate* s, int steps, int batch, float lr, uns
 /* Render one frame with the surrogate: same buffers and result layout as
  * launchRenderPipeline.  Requires an orbit camera (looking at the hole, no
  * roll: camRight.y == 0) and accumMode 0.  Two forms (bhSurrogateSetAnchors):
- *  - anchored (the default, anchor stride 4): the FP32 RK4 tracer traces one
+ *  - anchored (the default, anchor stride 8): the FP32 RK4 tracer traces one
  *    pixel in stride x stride (the anchors); a pixel between anchors takes the
  *    bicubic interpolation of the 4 x 4 surrounding anchors' escape directions
  *    when all 16 escaped without touching the disk, the network gives its cell
@@ -144,7 +144,7 @@ cudaError_t bhSurrogateRender(BHSurrogate* s, uchar4* out, float4* accum, float4
  * accuracy for speed; heldStride 1 compares every resolved pixel. */
 cudaError_t bhSurrogateSetGate(BHSurrogate* s, float minProb, float minConf, float critBand, int heldStride);
 
-/* Form of bhSurrogateRender (defaults 4, 1, 1e-4, 0.5): anchor stride (0:
+/* Form of bhSurrogateRender (defaults 8, 1, 1e-4, 0.5): anchor stride (0:
  * the network form; else 2..64), whether the network's cell gate applies,
  * the largest escape-direction error bound (rad) an interpolated pixel may
  * have, and the largest display-value change (in byte steps) allowed within

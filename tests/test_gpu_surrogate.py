@@ -332,8 +332,8 @@ def test_trained_surrogate_gain_over_plain_rk4(cuda, derive):
             return t, 1.0 - st[1] / st[0], float((d <= 1).mean())
 
         strict = (0.95, 0.95, 0.02, 256)
-        t_anc, res_anc, q_anc = run(net, 4, 1, strict)
-        t_anc0, res_anc0, q_anc0 = run(net, 4, 0, strict)
+        t_anc, res_anc, q_anc = run(net, 8, 1, strict)
+        t_anc0, res_anc0, q_anc0 = run(net, 8, 0, strict)
         t_perm, res_perm, q_perm = run(net, 0, 1, (0.5, 0.0, 0.02, 256))
         t_strict, res_strict, q_strict = run(net, 0, 1, strict)
         t_raw, res_raw, q_raw = run(raw, 0, 1, (0.5, 0.0, 0.02, 256))
