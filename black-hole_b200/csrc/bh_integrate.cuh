@@ -321,7 +321,7 @@ struct SphRay
         }
         phi += h;
 
-        if (!finite_p(u) || !finite_p(du)) { horizon = true; return true; }
+        if (!finite_p(u + du)) { horizon = true; return true; }   // either non-finite (u, du stay far below the float range)
         if (u >= F.uHor) { horizon = true; return true; }
         if (u < R(1e-4f)) { escaped = true; return true; }   // previous chord direction
 
@@ -675,7 +675,10 @@ struct KerrRay
     {
         const CamFrame<R>& F = frame_of<R>(P);
         if (step >= P.maxSteps) { exhaust(P); return true; }
-        if (!finite_p(r) || !finite_p(pr) || !finite_p(pth) || !finite_p(d1.r) || !finite_p(d1.pr))
+        // the reference's five finiteness tests (trace.cuh:757-760) as one: a NaN or
+        // infinity in any of them makes the sum non-finite (finite values of these
+        // quantities stay far below the float range)
+        if (!finite_p(((r + pr) + (pth + d1.r)) + d1.pr))
         { horizon = true; return true; }
         if (r <= F.capR) { horizon = true; return true; }
         if (STATS && r > F.rFloor105)
