@@ -11,7 +11,7 @@
 //     smooth), plus a floor of 2e-6 rad;
 //   * the pixel is accepted only if all 16 anchors escaped without touching
 //     the disk, the optional cell gate (the network's probability that the
-//     cell centre escapes without the disk) passes, the bound is below
+//     cell centre escapes without the disk, >= minProb) passes, the bound is below
 //     epsMax, and the sky is flat within the bound: either no star of the
 //     four star lattices lies within reach of the bound (an exact test on the
 //     lattice cell and the cell's star), or the display values (exposure,
@@ -20,6 +20,9 @@
 //     than maxStep; and the pixel stays below the bloom bright-pass
 //     threshold, so neither its byte nor its neighbours' bloom can move by
 //     a whole step;
+//   * a pixel whose 16 surrounding anchors were all captured without touching
+//     the disk (the inside of the shadow), and whose cell centre the network
+//     (when it gates) also calls captured, is black, as a captured sample is;
 //   * everything else goes on the RK4 list.
 // The sky is the reference's backgroundColor (trace.cuh:166-195) at the
 // interpolated direction, times the transmittance 1 of a sky-only ray
@@ -152,8 +155,13 @@ __global__ void __launch_bounds__(256) anchor_resolve_kernel(const __grid_consta
         }
         else if (cx >= 1 && cy >= 1 && cx + 2 < F.nx && cy + 2 < F.ny)
         {
-            bool sky = true;
-            if (F.cellGate) sky = F.cellGate[cy * (F.nx - 1) + cx].x >= F.minProb;
+            bool sky = true, dark = true;
+            if (F.cellGate)
+            {   // the network's class probabilities at the cell centre
+                const float2 g = F.cellGate[cy * (F.nx - 1) + cx];
+                sky = g.x >= F.minProb;
+                dark = g.y >= F.minProb;
+            }
             f3 d[4][4];
 #pragma unroll
             for (int j = 0; j < 4; ++j)
@@ -162,10 +170,18 @@ __global__ void __launch_bounds__(256) anchor_resolve_kernel(const __grid_consta
                 {   // anchor (cx - 1 + i, cy - 1 + j), staged at (cy - 1 + j - ay0, cx - 1 + i - ax0)
                     const float4 a = sAnc[cy - 1 + j - ay0][cx - 1 + i - ax0];
                     sky = sky && __float_as_uint(a.w) == BH_ANCHOR_ESCAPED;
+                    dark = dark && __float_as_uint(a.w) == BH_ANCHOR_HORIZON;
                     d[j][i] = v3(a.x, a.y, a.z);
                 }
             reason = 1;
-            if (sky)
+            if (dark)
+            {   // inside the shadow: all 16 anchors captured without touching the disk, and a
+                // captured ray's sample is exactly zero (renderSampleHDR, trace.cuh:916-921)
+                hdr = v3(0.f, 0.f, 0.f);
+                resolved = true;
+                reason = 0;
+            }
+            else if (sky)
             {
                 const float tx = (float)(x - cx * S) / (float)S, ty = (float)(y - cy * S) / (float)S;
                 float wx[4], wy[4];

@@ -349,12 +349,14 @@ sg_infer_kernel(const __grid_constant__ CUtensorMap tW, const __grid_constant__ 
                 if constexpr (FRAME)
                 {
                     if (F.gateOut)
-                    {   // cell gate of an anchored frame: P(escaped without the disk), confidence
+                    {   // cell gate of an anchored frame: P(escaped without the disk),
+                        // P(captured without the disk)
                         if (valid)
                         {
                             const float m = fmaxf(y[0], fmaxf(y[1], y[2]));
                             const float e0 = __expf(y[0] - m), e1 = __expf(y[1] - m), e2 = __expf(y[2] - m);
-                            F.gateOut[rid] = make_float2(e0 / (e0 + e1 + e2), 1.f / (1.f + __expf(-y[kOConf])));
+                            const float inv = 1.f / (e0 + e1 + e2);
+                            F.gateOut[rid] = make_float2(e0 * inv, e1 * inv);
                         }
                     }
                     else frame_output(F, rid, valid, r, y);

@@ -29,7 +29,8 @@ struct SgFrame
     int heldStride;                 // 1 in heldStride surrogate pixels is held out (0: none)
     unsigned frameSeed;
     // cell-gate mode (anchored frames): ray k is pixel evalPix[k]; instead of deciding the
-    // pixel, the kernel writes (probability of "escaped without the disk", confidence) to gateOut[k]
+    // pixel, the kernel writes the probabilities of "escaped without the disk" and of
+    // "captured without the disk" to gateOut[k]
     const unsigned* evalPix;
     float2* gateOut;
 };
@@ -58,8 +59,8 @@ struct SgAnchorFrame
     TraceParams tp;
     const BHAnchor* anchors;
     int S, nx, ny;
-    const float2* cellGate;         // null, or per cell (nx - 1) x (ny - 1): (P(sky), confidence)
-    float minProb;                  // cell gate: P(escaped without the disk) needed at the cell centre
+    const float2* cellGate;         // null, or per cell (nx - 1) x (ny - 1): (P(sky), P(shadow))
+    float minProb;                  // cell gate: probability of the cell's class needed at its centre
     float epsMax;                   // largest interpolation error bound (rad) a pixel may have
     float maxStep;                  // sensitivity bar: display-value change (byte units) within the bound
     unsigned* list;

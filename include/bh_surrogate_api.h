@@ -124,7 +124,9 @@ cudaError_t bhSurrogateTrain(BHSurrogate* s, int steps, int batch, float lr, uns
  *    centre a probability >= minProb of escaping without the disk, the
  *    interpolation error bound is <= epsMax and the sky is flat within that
  *    bound (display values within maxStep of a byte step, below the bloom
- *    threshold); every other pixel is traced;
+ *    threshold); a pixel whose 16 anchors were all captured without the disk
+ *    (and whose cell centre the network calls captured) is black; every other
+ *    pixel is traced;
  *  - network (stride 0): the fused kernel resolves the pixels it is sure of
  *    from its own escape direction (escaped or captured without the disk,
  *    class probability and confidence >= 0.95, farther than 2 % from the
