@@ -99,29 +99,40 @@ __device__ __forceinline__ f3 unit3(f3 v)
     return v3(v.x * l, v.y * l, v.z * l);
 }
 
-__device__ __forceinline__ void push(unsigned* list, unsigned* count, unsigned pix, bool want)
+// Warp-wide append of one 8x4 tile's pixels that need RK4: a warp with any
+// claims a whole 32-entry group of the list, so the tracer's warps (which take
+// 32 consecutive entries) trace one tile each, as coherent as in the plain
+// frame; lanes without a pixel hold BH_PIX_SKIP.  `traced` counts the pixels.
+__device__ __forceinline__ void push_tile(unsigned* list, unsigned* count, unsigned* traced, unsigned pix,
+                                          bool want)
 {
     const unsigned lane = threadIdx.x & 31u;
     const unsigned m = __ballot_sync(0xffffffffu, want);
     if (!m) return;
     unsigned base = 0;
-    if (lane == (unsigned)(__ffs(m) - 1)) base = atomicAdd(count, (unsigned)__popc(m));
-    base = __shfl_sync(0xffffffffu, base, __ffs(m) - 1);
-    if (want) list[base + __popc(m & ((1u << lane) - 1u))] = pix;
+    if (lane == 0)
+    {
+        base = atomicAdd(count, 32u);
+        atomicAdd(traced, (unsigned)__popc(m));
+    }
+    base = __shfl_sync(0xffffffffu, base, 0);
+    list[base + lane] = want ? pix : BH_PIX_SKIP;
 }
 
 // anchors a 32 x 8 pixel block can reach: columns x0/S - 1 .. (x0+31)/S + 2, rows
 // y0/S - 1 .. (y0+7)/S + 2 (at most 19 x 8 for S >= 2)
 constexpr int kAncCols = 19, kAncRows = 8;
 
-// One thread per pixel; 2-D blocks of 32 x 8 pixels (the warp is one row of 32).
+// One thread per pixel; 2-D blocks of 32 x 8 pixels, each warp one 8 x 4 tile
+// (4 tiles across, 2 down).
 // The block's anchors (escape direction and flags) are staged in shared memory
 // once; each pixel then reads its 4 x 4 neighbourhood from there.
 __global__ void __launch_bounds__(256) anchor_resolve_kernel(const __grid_constant__ SgAnchorFrame F)
 {
     __shared__ float4 sAnc[kAncRows][kAncCols];
     const TraceParams& P = F.tp;
-    const int x = blockIdx.x * 32 + (threadIdx.x & 31), y = blockIdx.y * 8 + (threadIdx.x >> 5);
+    const int warp = threadIdx.x >> 5, lane = threadIdx.x & 31;
+    const int x = blockIdx.x * 32 + (warp & 3) * 8 + (lane & 7), y = blockIdx.y * 8 + (warp >> 2) * 4 + (lane >> 3);
     const bool inFrame = x < P.W && y < P.H;
     const int S = F.S;
     const unsigned pix = inFrame ? (unsigned)y * (unsigned)P.W + (unsigned)x : 0u;
@@ -254,13 +265,12 @@ __global__ void __launch_bounds__(256) anchor_resolve_kernel(const __grid_consta
         held = (h % (unsigned)F.heldStride) == 0u;
     }
     const bool trace = inFrame && !anchor && !resolved;
-    push(F.list, F.listCount, pix, trace || held);
-    const unsigned lane = threadIdx.x & 31u;
+    push_tile(F.list, F.listCount, F.stats + 4, pix, trace || held);
     const unsigned mh = __ballot_sync(0xffffffffu, held);
     if (mh)
     {
         unsigned base = 0;
-        if (lane == (unsigned)(__ffs(mh) - 1)) base = atomicAdd(F.heldCount, (unsigned)__popc(mh));
+        if (lane == __ffs(mh) - 1) base = atomicAdd(F.heldCount, (unsigned)__popc(mh));
         base = __shfl_sync(0xffffffffu, base, __ffs(mh) - 1);
         if (held)
         {

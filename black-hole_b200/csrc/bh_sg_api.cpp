@@ -208,21 +208,26 @@ cudaError_t criticalCurve(BHSurrogate* s, const RenderParams& P0, float* crit)
     return e;
 }
 
-cudaError_t ensureFrame(BHSurrogate* s, size_t pixels)
+// Frame scratch of a W x H frame.  The RK4 list holds whole 32-entry groups:
+// 8x4 tiles in the anchored form, 32 consecutive pixels in the network form, so
+// its length is bounded by the frame padded to whole tiles or whole groups.
+cudaError_t ensureFrame(BHSurrogate* s, int W, int H)
 {
+    const size_t pixels = (size_t)W * H;
+    const size_t listLen = std::max((size_t)((W + 7) / 8 * 8) * (size_t)((H + 3) / 4 * 4), (pixels + 31) / 32 * 32);
     const size_t stride = s->heldStride > 0 ? (size_t)s->heldStride : pixels + 1;
     const size_t want = std::min(pixels, pixels / stride * 2 + 4096);
-    if (pixels <= s->listCap && want <= s->heldCap) return cudaSuccess;
+    if (listLen <= s->listCap && want <= s->heldCap) return cudaSuccess;
     if (s->list) cudaFree(s->list);
     if (s->heldPix) cudaFree(s->heldPix);
     if (s->heldPred) cudaFree(s->heldPred);
     s->list = nullptr; s->heldPix = nullptr; s->heldPred = nullptr; s->listCap = 0; s->heldCap = 0;
     const unsigned cap = (unsigned)want;
-    cudaError_t e = bh_device_alloc(reinterpret_cast<void**>(&s->list), pixels * sizeof(unsigned));
+    cudaError_t e = bh_device_alloc(reinterpret_cast<void**>(&s->list), listLen * sizeof(unsigned));
     if (e == cudaSuccess) e = bh_device_alloc(reinterpret_cast<void**>(&s->heldPix), cap * sizeof(unsigned));
     if (e == cudaSuccess) e = bh_device_alloc(reinterpret_cast<void**>(&s->heldPred), cap * sizeof(float4));
     if (e != cudaSuccess) return e;
-    s->listCap = pixels;
+    s->listCap = listLen;
     s->heldCap = cap;
     return cudaSuccess;
 }
@@ -307,7 +312,7 @@ cudaError_t anchoredFrame(BHSurrogate* s, const RenderParams& P, float4* accum, 
     A.heldCap = s->heldCap;
     A.heldStride = s->heldStride;
     A.frameSeed = ++s->frames;
-    A.stats = s->counters + 8;
+    A.stats = s->counters + 8;      // [8..11] tallies, [12] pixels on the list
     s->lastAnchors = nA;
     return sg_anchor_resolve(A, stream);
 }
@@ -562,7 +567,7 @@ cudaError_t bhSurrogateRender(BHSurrogate* s, uchar4* out, float4* accum, float4
     if (!out || !accum || (P.bloomEnabled && (!bloomA || !bloomB))) return cudaErrorInvalidValue;
     if (std::fabs(P.camRight.y) > 1e-4f || P.accumMode != 0) return cudaErrorInvalidValue;
     const size_t pixels = (size_t)P.width * P.height;
-    cudaError_t e = ensureFrame(s, pixels);
+    cudaError_t e = ensureFrame(s, P.width, P.height);
     if (e != cudaSuccess) return e;
     s->lastPixels = (unsigned)pixels;
     if (s->anchorStride >= 2)
@@ -592,6 +597,7 @@ cudaError_t bhSurrogateRender(BHSurrogate* s, uchar4* out, float4* accum, float4
     F.minConf = s->minConf;
     F.list = s->list;
     F.listCount = s->counters;
+    F.traced = s->counters + 12;
     F.heldPix = s->heldPix;
     F.heldPred = s->heldPred;
     F.heldCount = s->counters + 1;
@@ -613,7 +619,6 @@ cudaError_t bhSurrogateFrameStats(BHSurrogate* s, BHSurrogateStats* st)
     if (e == cudaSuccess) e = checkErrWord(s);
     if (e != cudaSuccess) return e;
     st->pixels = s->lastPixels;
-    st->rk4Pixels = c[0];
     st->heldOut = c[4];
     st->heldOutOver1Lsb = c[5];
     float mx;
@@ -621,7 +626,7 @@ cudaError_t bhSurrogateFrameStats(BHSurrogate* s, BHSurrogateStats* st)
     st->heldOutMaxAbs = mx;
     st->heldOutOverTol = c[7];
     st->anchors = s->lastAnchors;
-    st->rk4Pixels += s->lastAnchors;
+    st->rk4Pixels = c[12] + s->lastAnchors;   // pixels on the list (padded to groups) + anchors
     st->interpolated = c[8];
     st->rejectAnchors = c[9];
     st->rejectBound = c[10];

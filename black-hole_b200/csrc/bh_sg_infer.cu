@@ -141,16 +141,23 @@ __device__ void frame_output(const SgFrame& F, unsigned pix, bool valid, const R
             acc[pix] = make_float4(hdr.x, hdr.y, hdr.z, 1.f);
         }
     }
-    // warp-aggregated appends to the RK4 list (fallback and held-out pixels)
+    // appends to the RK4 list (fallback and held-out pixels): a warp's lanes are 32
+    // consecutive pixels of a row, and a warp with any claims a whole 32-entry group
+    // (BH_PIX_SKIP where a lane has none), so each tracing warp takes one coherent
+    // row segment
     const unsigned lane = threadIdx.x & 31u;
     const bool push = fallback || held;
     const unsigned m = __ballot_sync(0xffffffffu, push);
     if (m)
     {
         unsigned base = 0;
-        if (lane == (unsigned)(__ffs(m) - 1)) base = atomicAdd(F.listCount, (unsigned)__popc(m));
-        base = __shfl_sync(0xffffffffu, base, __ffs(m) - 1);
-        if (push) F.list[base + __popc(m & ((1u << lane) - 1u))] = pix;
+        if (lane == 0)
+        {
+            base = atomicAdd(F.listCount, 32u);
+            atomicAdd(F.traced, (unsigned)__popc(m));
+        }
+        base = __shfl_sync(0xffffffffu, base, 0);
+        F.list[base + lane] = push ? pix : BH_PIX_SKIP;
     }
     const unsigned mh = __ballot_sync(0xffffffffu, held);
     if (mh)

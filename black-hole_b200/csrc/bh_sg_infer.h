@@ -20,8 +20,9 @@ struct SgFrame
     float crit[kCritBins];          // critical screen radius (tan units) per polar angle bin
     float critBand;                 // relative half-width of the RK4 band around it
     float minProb, minConf;         // class probability / confidence needed to keep a pixel
-    unsigned* list;                 // RK4 pixel list (capacity W * H)
-    unsigned* listCount;
+    unsigned* list;                 // RK4 pixel list, in 32-entry groups (BH_PIX_SKIP pads a group)
+    unsigned* listCount;            // entries of the list (padding included)
+    unsigned* traced;               // pixels on the list
     unsigned* heldPix;              // held-out sample: pixel and surrogate HDR
     float4* heldPred;
     unsigned* heldCount;
@@ -72,7 +73,8 @@ struct SgAnchorFrame
     int heldStride;
     unsigned frameSeed;
     unsigned* stats;                // [0] interpolated, [1] rejected by the anchors / cell gate,
-                                    // [2] by the error bound, [3] by the sky sensitivity
+                                    // [2] by the error bound, [3] by the sky sensitivity,
+                                    // [4] pixels on the list (the list itself is padded to tiles)
 };
 
 cudaError_t sg_anchor_resolve(const SgAnchorFrame& F, cudaStream_t s);

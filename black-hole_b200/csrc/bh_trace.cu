@@ -40,11 +40,11 @@ template <class R, int NW> struct Queue<R, true, NW> { PackedRay<R> s[NW][kQueue
 BH_DEV bool ray_pixel(const TraceParams& P, unsigned rid, int& px, int& py)
 {
     if (P.pixList)
-    {
+    {   // BH_PIX_SKIP entries pad a list group: no ray
         const unsigned pix = __ldg(P.pixList + rid);
         py = (int)(pix / (unsigned)P.W);
         px = (int)(pix - (unsigned)py * (unsigned)P.W);
-        return true;
+        return pix != BH_PIX_SKIP;
     }
     unsigned tile = rid >> 5, w = rid & 31u;
     if (P.tileOrder) tile = __ldg(P.tileOrder + tile);

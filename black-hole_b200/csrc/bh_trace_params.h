@@ -30,6 +30,9 @@ struct BHAnchor
 };
 enum { BH_ANCHOR_ESCAPED = 1u, BH_ANCHOR_HORIZON = 2u, BH_ANCHOR_DISK = 4u };
 
+// pixel-list entry that traces nothing (pads a 32-entry group of a list)
+constexpr unsigned BH_PIX_SKIP = 0xFFFFFFFFu;
+
 // Camera-frame quantities shared by every ray of a view, in the integration
 // precision T.  They are the per-ray prologue of the reference integrators
 // (src/trace.cuh:213-247, 490-521, 703-739 of Sqhh99/Black-hole) with

@@ -248,25 +248,29 @@ def test_render_with_every_pixel_on_rk4_equals_plain_frame(cuda, derive, stride)
         net.close()
 
 
-def test_anchored_frame_within_one_lsb_of_plain(cuda, derive):
-    """Anchored form without the network gate: RK4 anchors every 4 pixels, the
-    rest interpolated where the error bound and the sky allow.  Most pixels are
-    interpolated, every pixel stays within +-1 LSB of the plain frame on >= 99.9 %
-    of pixels, anchors equal the plain frame bit for bit, and the tallies add up."""
+@pytest.mark.parametrize("w,h,stride,min_interp", [(960, 540, 4, 0.5), (960, 540, 8, 0.5),
+                                                   (333, 197, 8, 0.2)])   # ragged: tiles padded
+def test_anchored_frame_within_one_lsb_of_plain(cuda, derive, w, h, stride, min_interp):
+    """Anchored form without the network gate: RK4 anchors every `stride` pixels,
+    the rest interpolated (or black inside the shadow) where the error bound and
+    the sky allow.  Most pixels are not traced, the frame is within +-1 LSB of the
+    plain frame on >= 99.9 % of pixels, anchors and traced pixels equal the plain
+    frame's bit for bit, and the tallies add up."""
     net = Net(5)
     try:
-        _anchors(net, 4, use_net=0)
-        P = _kn_scene(derive, 960, 540, az=75.0)
+        _anchors(net, stride, use_net=0)
+        P = _kn_scene(derive, w, h, az=75.0)
         out, acc, st = _render(net, P)
         pout, pacc = _plain(P)
-        n = 960 * 540
+        n = w * h
         d = np.abs(out[..., :3].astype(int) - pout[..., :3].astype(int)).max(-1)
         anchors = int(st[6])
         print("stats", st, "within 1 LSB", float((d <= 1).mean()), "exact", float((d == 0).mean()))
-        assert anchors == ((960 - 1) // 4 + 1) * ((540 - 1) // 4 + 1)
-        assert np.array_equal(acc[::4, ::4], pacc[::4, ::4])          # anchors are plain-frame pixels
-        assert st[7] > 0.5 * n                                        # interpolated
+        assert anchors == ((w - 1) // stride + 1) * ((h - 1) // stride + 1)
+        assert np.array_equal(acc[::stride, ::stride], pacc[::stride, ::stride])   # anchors: plain pixels
+        assert st[7] > min_interp * n                                 # interpolated (or shadow)
         assert st[7] + st[8] + st[9] + st[10] + anchors == n           # every pixel accounted for once
+        assert st[1] == n - st[7] + st[2]                              # traced: the rest + held-out
         assert float((d <= 1).mean()) >= 0.999
         assert st[3] <= max(2, st[2] // 100)                           # held-out sample over 1 LSB
     finally:
