@@ -145,7 +145,7 @@ __global__ void __launch_bounds__(256) anchor_resolve_kernel(const __grid_consta
         float4 v = make_float4(0.f, 0.f, 0.f, 0.f);
         if (ax >= 0 && ay >= 0 && ax < F.nx && ay < F.ny)
         {
-            const BHAnchor& a = F.anchors[ay * F.nx + ax];
+            const BHAnchor& a = F.anchors[F.slot[ay * F.nx + ax]];
             v = make_float4(a.escDir.x, a.escDir.y, a.escDir.z, __uint_as_float(a.flags));
         }
         sAnc[r][c] = v;
@@ -160,7 +160,7 @@ __global__ void __launch_bounds__(256) anchor_resolve_kernel(const __grid_consta
         const int cx = x / S, cy = y / S;
         if (x == cx * S && y == cy * S)
         {   // an anchor: its own RK4 sample
-            const BHAnchor& a = F.anchors[cy * F.nx + cx];
+            const BHAnchor& a = F.anchors[F.slot[cy * F.nx + cx]];
             hdr = v3(a.hdr.x, a.hdr.y, a.hdr.z);
             anchor = true;
         }
@@ -265,7 +265,7 @@ __global__ void __launch_bounds__(256) anchor_resolve_kernel(const __grid_consta
         held = (h % (unsigned)F.heldStride) == 0u;
     }
     const bool trace = inFrame && !anchor && !resolved;
-    push_tile(F.list, F.listCount, F.stats + 4, pix, trace || held);
+    push_tile(F.list, F.listCount, F.stats + 4, pix, trace);   // held-out pixels: traced from heldPix
     const unsigned mh = __ballot_sync(0xffffffffu, held);
     if (mh)
     {

@@ -104,7 +104,8 @@ struct BHSurrogate
     // frame scratch
     unsigned* list = nullptr;
     size_t listCap = 0;
-    unsigned* counters = nullptr;     // [0] RK4 list size, [1] held-out count, [4..7] held-out statistics
+    unsigned* counters = nullptr;     // [0] RK4 list groups x 32, [1] held-out count, [4..7] held-out statistics,
+                                      // [8..11] anchored tallies, [12] listed pixels, [13] list + held-out length
     unsigned* heldPix = nullptr;
     float4* heldPred = nullptr;
     unsigned heldCap = 0;
@@ -126,7 +127,8 @@ struct BHSurrogate
     bool anchorNet = true;
     float epsMax = 1e-4f, maxStep = 0.5f;
     int aW = 0, aH = 0, aS = 0, aNx = 0, aNy = 0;
-    unsigned* anchorPix = nullptr;    // anchor pixels, row-major
+    unsigned* anchorPix = nullptr;    // anchor pixels in trace order
+    unsigned* anchorSlot = nullptr;   // anchor (ax, ay) -> its index in anchorPix / anchorRec
     BHAnchor* anchorRec = nullptr;
     unsigned* cellPix = nullptr;      // cell-centre pixels
     float2* cellGate = nullptr;
@@ -141,8 +143,8 @@ void freeAll(BHSurrogate* s)
     SgState& S = s->S;
     sg_free_batch(S);
     void* ps[] = {S.params, S.grads, S.adamM, S.adamV, S.W, S.Wt, S.biasPacked, S.loss, S.dsIn, S.dsTgt, s->list,
-                  s->counters, s->heldPix, s->heldPred, s->bIn, s->bTgt, s->anchorPix, s->anchorRec, s->cellPix,
-                  s->cellGate};
+                  s->counters, s->heldPix, s->heldPred, s->bIn, s->bTgt, s->anchorPix, s->anchorSlot, s->anchorRec,
+                  s->cellPix, s->cellGate};
     for (void* p : ps)
         if (p) cudaFree(p);
     if (s->stream) cudaStreamDestroy(s->stream);
@@ -208,15 +210,17 @@ cudaError_t criticalCurve(BHSurrogate* s, const RenderParams& P0, float* crit)
     return e;
 }
 
-// Frame scratch of a W x H frame.  The RK4 list holds whole 32-entry groups:
-// 8x4 tiles in the anchored form, 32 consecutive pixels in the network form, so
-// its length is bounded by the frame padded to whole tiles or whole groups.
+// Frame scratch of a W x H frame.  The RK4 list holds whole 32-entry groups
+// (8x4 tiles in the anchored form, 32 consecutive pixels in the network form),
+// bounded by the frame padded to whole tiles or whole groups, followed by the
+// held-out sample (at most heldCap pixels).
 cudaError_t ensureFrame(BHSurrogate* s, int W, int H)
 {
     const size_t pixels = (size_t)W * H;
-    const size_t listLen = std::max((size_t)((W + 7) / 8 * 8) * (size_t)((H + 3) / 4 * 4), (pixels + 31) / 32 * 32);
     const size_t stride = s->heldStride > 0 ? (size_t)s->heldStride : pixels + 1;
     const size_t want = std::min(pixels, pixels / stride * 2 + 4096);
+    const size_t listLen =
+        std::max((size_t)((W + 7) / 8 * 8) * (size_t)((H + 3) / 4 * 4), (pixels + 31) / 32 * 32) + want;
     if (listLen <= s->listCap && want <= s->heldCap) return cudaSuccess;
     if (s->list) cudaFree(s->list);
     if (s->heldPix) cudaFree(s->heldPix);
@@ -234,7 +238,9 @@ cudaError_t ensureFrame(BHSurrogate* s, int W, int H)
 
 // Anchor lattice of a W x H frame: pixels (S ax, S ay), and the centres of the
 // (nx - 1) x (ny - 1) cells between them; built once per size and stride
-// (blocking upload).
+// (blocking upload).  The anchors are traced in 8x4 groups of neighbouring
+// anchors (one tracing warp each), groups nearest the screen centre first as
+// in the plain frame's tile order, so the long rays near the shadow start early.
 cudaError_t ensureAnchors(BHSurrogate* s, int W, int H, int S)
 {
     if (s->aW == W && s->aH == H && s->aS == S && s->anchorPix) return cudaSuccess;
@@ -244,9 +250,11 @@ cudaError_t ensureAnchors(BHSurrogate* s, int W, int H, int S)
     if (nA > s->aCap)
     {
         if (s->anchorPix) cudaFree(s->anchorPix);
+        if (s->anchorSlot) cudaFree(s->anchorSlot);
         if (s->anchorRec) cudaFree(s->anchorRec);
-        s->anchorPix = nullptr; s->anchorRec = nullptr; s->aCap = 0;
+        s->anchorPix = nullptr; s->anchorSlot = nullptr; s->anchorRec = nullptr; s->aCap = 0;
         if ((e = bh_device_alloc(reinterpret_cast<void**>(&s->anchorPix), nA * sizeof(unsigned)))) return e;
+        if ((e = bh_device_alloc(reinterpret_cast<void**>(&s->anchorSlot), nA * sizeof(unsigned)))) return e;
         if ((e = bh_device_alloc(reinterpret_cast<void**>(&s->anchorRec), nA * sizeof(BHAnchor)))) return e;
         s->aCap = nA;
     }
@@ -259,13 +267,32 @@ cudaError_t ensureAnchors(BHSurrogate* s, int W, int H, int S)
         if ((e = bh_device_alloc(reinterpret_cast<void**>(&s->cellGate), nC * sizeof(float2)))) return e;
         s->cCap = nC;
     }
-    std::vector<unsigned> a(nA), c(nC, 0u);
-    for (int y = 0; y < ny; ++y)
-        for (int x = 0; x < nx; ++x) a[(size_t)y * nx + x] = (unsigned)(y * S) * (unsigned)W + (unsigned)(x * S);
+    const int gx = (nx + 7) / 8, gy = (ny + 3) / 4;
+    std::vector<unsigned> groups((size_t)gx * gy);
+    std::vector<float> key(groups.size());
+    for (size_t g = 0; g < groups.size(); ++g)
+    {
+        groups[g] = (unsigned)g;
+        const float dx = ((float)(g % gx) * 8.f + 3.5f) * S - 0.5f * W, dy = ((float)(g / gx) * 4.f + 1.5f) * S - 0.5f * H;
+        key[g] = dx * dx + dy * dy;
+    }
+    std::stable_sort(groups.begin(), groups.end(), [&](unsigned p, unsigned q) { return key[p] < key[q]; });
+    std::vector<unsigned> a, slot(nA), c(nC, 0u);
+    a.reserve(nA);
+    for (unsigned g : groups)
+        for (int j = 0; j < 4; ++j)
+            for (int i = 0; i < 8; ++i)
+            {
+                const int x = (int)(g % gx) * 8 + i, y = (int)(g / gx) * 4 + j;
+                if (x >= nx || y >= ny) continue;
+                slot[(size_t)y * nx + x] = (unsigned)a.size();
+                a.push_back((unsigned)(y * S) * (unsigned)W + (unsigned)(x * S));
+            }
     for (int y = 0; y + 1 < ny; ++y)
         for (int x = 0; x + 1 < nx; ++x)
             c[(size_t)y * (nx - 1) + x] = (unsigned)(y * S + S / 2) * (unsigned)W + (unsigned)(x * S + S / 2);
     if ((e = cudaMemcpy(s->anchorPix, a.data(), nA * sizeof(unsigned), cudaMemcpyHostToDevice))) return e;
+    if ((e = cudaMemcpy(s->anchorSlot, slot.data(), nA * sizeof(unsigned), cudaMemcpyHostToDevice))) return e;
     if ((e = cudaMemcpy(s->cellPix, c.data(), nC * sizeof(unsigned), cudaMemcpyHostToDevice))) return e;
     s->aW = W; s->aH = H; s->aS = S; s->aNx = nx; s->aNy = ny;
     return cudaSuccess;
@@ -299,6 +326,7 @@ cudaError_t anchoredFrame(BHSurrogate* s, const RenderParams& P, float4* accum, 
     SgAnchorFrame A{};
     A.tp = bh_frame_params(P, BH_OUT_ACCUM, accum);
     A.anchors = s->anchorRec;
+    A.slot = s->anchorSlot;
     A.S = S; A.nx = s->aNx; A.ny = s->aNy;
     A.cellGate = s->anchorNet ? s->cellGate : nullptr;
     A.minProb = s->minProb;
@@ -317,17 +345,20 @@ cudaError_t anchoredFrame(BHSurrogate* s, const RenderParams& P, float4* accum, 
     return sg_anchor_resolve(A, stream);
 }
 
-// RK4 for the listed pixels (the tracer reads the list and its device-side
-// length), the held-out comparison, then bloom and tonemap.
+// RK4 for the listed pixels and, after them, the held-out sample (the tracer
+// reads the list and its device-side length), the held-out comparison, then
+// bloom and tonemap.
 cudaError_t traceListAndPost(BHSurrogate* s, const RenderParams& P, uchar4* out, float4* accum, float4* bloomA,
                              float4* bloomB, cudaStream_t stream)
 {
+    cudaError_t e = sg_append_held(s->list, s->counters, s->heldPix, s->counters + 1, s->heldCap, s->counters + 13,
+                                   stream);
+    if (e != cudaSuccess) return e;
     TraceParams t = bh_frame_params(P, BH_OUT_ACCUM, accum);
     t.pixList = s->list;
-    t.nRaysDev = s->counters;
-    t.nRays = (unsigned)((size_t)P.width * P.height);
-    cudaError_t e = bh_device_counter(&t.counter);
-    if (e != cudaSuccess) return e;
+    t.nRaysDev = s->counters + 13;
+    t.nRays = (unsigned)s->listCap;
+    if ((e = bh_device_counter(&t.counter)) != cudaSuccess) return e;
     if ((e = bh_launch_trace(t, BH_PREC_FP32, false, bh_family_blocks(P), stream)) != cudaSuccess) return e;
     if ((e = sg_held_compare(accum, s->heldPix, s->heldPred, s->counters + 1, s->heldCap, t, s->counters + 4,
                              stream)) != cudaSuccess)
@@ -626,7 +657,7 @@ cudaError_t bhSurrogateFrameStats(BHSurrogate* s, BHSurrogateStats* st)
     st->heldOutMaxAbs = mx;
     st->heldOutOverTol = c[7];
     st->anchors = s->lastAnchors;
-    st->rk4Pixels = c[12] + s->lastAnchors;   // pixels on the list (padded to groups) + anchors
+    st->rk4Pixels = c[12] + std::min(c[1], s->heldCap) + s->lastAnchors;   // listed + held-out + anchors
     st->interpolated = c[8];
     st->rejectAnchors = c[9];
     st->rejectBound = c[10];

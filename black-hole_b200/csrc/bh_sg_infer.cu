@@ -141,12 +141,12 @@ __device__ void frame_output(const SgFrame& F, unsigned pix, bool valid, const R
             acc[pix] = make_float4(hdr.x, hdr.y, hdr.z, 1.f);
         }
     }
-    // appends to the RK4 list (fallback and held-out pixels): a warp's lanes are 32
-    // consecutive pixels of a row, and a warp with any claims a whole 32-entry group
-    // (BH_PIX_SKIP where a lane has none), so each tracing warp takes one coherent
-    // row segment
+    // appends to the RK4 list (fallback pixels; the held-out sample follows the list,
+    // sg_append_held): a warp's lanes are 32 consecutive pixels of a row, and a warp
+    // with any claims a whole 32-entry group (BH_PIX_SKIP where a lane has none), so
+    // each tracing warp takes one coherent row segment
     const unsigned lane = threadIdx.x & 31u;
-    const bool push = fallback || held;
+    const bool push = fallback;
     const unsigned m = __ballot_sync(0xffffffffu, push);
     if (m)
     {
@@ -456,7 +456,24 @@ __global__ void held_compare_kernel(const float4* __restrict__ accum, const unsi
     if (d > 1e-3f * fmaxf(ref, 1e-3f)) atomicAdd(stats + 3, 1u);
 }
 
+__global__ void append_held_kernel(unsigned* __restrict__ list, const unsigned* __restrict__ listCount,
+                                   const unsigned* __restrict__ heldPix, const unsigned* __restrict__ heldCount,
+                                   unsigned heldCap, unsigned* __restrict__ total)
+{
+    const unsigned base = *listCount, n = min(*heldCount, heldCap);
+    for (unsigned k = blockIdx.x * blockDim.x + threadIdx.x; k < n; k += gridDim.x * blockDim.x)
+        list[base + k] = heldPix[k];
+    if (blockIdx.x == 0 && threadIdx.x == 0) *total = base + n;
+}
+
 }  // namespace
+
+cudaError_t sg_append_held(unsigned* list, const unsigned* listCount, const unsigned* heldPix,
+                           const unsigned* heldCount, unsigned heldCap, unsigned* total, cudaStream_t s)
+{
+    append_held_kernel<<<32, 256, 0, s>>>(list, listCount, heldPix, heldCount, heldCap, total);
+    return cudaGetLastError();
+}
 
 cudaError_t sg_held_compare(const float4* accum, const unsigned* heldPix, const float4* heldPred,
                             const unsigned* heldCount, unsigned heldCap, const TraceParams& tp, unsigned* stats,

@@ -52,13 +52,15 @@ cudaError_t sg_infer_launch(const SgInferArgs& a, const SgFrame* frame, cudaStre
 
 // Anchored surrogate frame (bh_sg_anchor.cu).  The anchors are the pixels
 // (S ax, S ay), ax < nx = (W - 1) / S + 1, ay < ny = (H - 1) / S + 1, traced
-// by RK4 into `anchors` (row-major, BH_OUT_ANCHOR records).  The resolve pass
-// writes every anchor's HDR and every pixel it can interpolate to the
-// accumulation buffer (tp.out) and appends the rest to `list`.
+// by RK4 into `anchors` (BH_OUT_ANCHOR records, in trace order).  The resolve
+// pass writes every anchor's HDR and every pixel it can interpolate to the
+// accumulation buffer (tp.out), appends the pixels to trace to `list` in
+// whole 8x4 tiles, and records the held-out sample in heldPix.
 struct SgAnchorFrame
 {
     TraceParams tp;
-    const BHAnchor* anchors;
+    const BHAnchor* anchors;        // in trace order (8x4 anchor tiles, centre-out)
+    const unsigned* slot;           // anchor (ax, ay) -> its record: slot[ay * nx + ax]
     int S, nx, ny;
     const float2* cellGate;         // null, or per cell (nx - 1) x (ny - 1): (P(sky), P(shadow))
     float minProb;                  // cell gate: probability of the cell's class needed at its centre
@@ -74,15 +76,23 @@ struct SgAnchorFrame
     unsigned frameSeed;
     unsigned* stats;                // [0] interpolated, [1] rejected by the anchors / cell gate,
                                     // [2] by the error bound, [3] by the sky sensitivity,
-                                    // [4] pixels on the list (the list itself is padded to tiles)
+                                    // [4] pixels on the list (the list itself is padded to tiles;
+                                    // held-out pixels are not on it)
 };
 
 cudaError_t sg_anchor_resolve(const SgAnchorFrame& F, cudaStream_t s);
 
+// Appends the held-out sample (heldPix[0, min(*heldCount, heldCap))) to the RK4
+// list after its *listCount entries and writes the total length to *total, so
+// one tracer launch traces both: the sampled pixels fill the end of the launch
+// instead of each claiming a tracing warp in its own tile.
+cudaError_t sg_append_held(unsigned* list, const unsigned* listCount, const unsigned* heldPix,
+                           const unsigned* heldCount, unsigned heldCap, unsigned* total, cudaStream_t s);
+
 // Held-out comparison after the RK4 pass: stats[0] += pixels compared,
 // stats[1] += pixels whose RGBA8 (exposure, no bloom) differs by more than
-// 1 LSB, stats[2] = max |HDR difference| (float bits), stats[3] += escaped
-// class disagreements (RK4 pixel not sky-only).
+// 1 LSB, stats[2] = max |HDR difference| (float bits), stats[3] += pixels whose
+// HDR differs by more than 1e-3 relative (floor 1e-3).
 cudaError_t sg_held_compare(const float4* accum, const unsigned* heldPix, const float4* heldPred,
                             const unsigned* heldCount, unsigned heldCap, const TraceParams& tp, unsigned* stats,
                             cudaStream_t s);

@@ -173,7 +173,7 @@ trace_kernel(const __grid_constant__ TraceParams P)
     const unsigned FULL = 0xffffffffu, below = (1u << lane) - 1u;
     PackedRay<R>* ring = Q.s[warp];
 
-    const unsigned nRays = P.nRaysDev ? *P.nRaysDev : P.nRays;
+    const unsigned nRays = P.nRaysDev ? min(*P.nRaysDev, P.nRays) : P.nRays;
     Ray ray;
     unsigned rid = 0, key = 0;
     bool live = false;
@@ -315,7 +315,7 @@ __global__ void __launch_bounds__(block_of<Ray, false>(), min_blocks<Ray, false>
 tile_kernel(const __grid_constant__ TraceParams P)
 {
     const unsigned lane = threadIdx.x & 31u;
-    const unsigned nRays = P.nRaysDev ? *P.nRaysDev : P.nRays;
+    const unsigned nRays = P.nRaysDev ? min(*P.nRaysDev, P.nRays) : P.nRays;
     const unsigned nTiles = (nRays + 31u) / 32u;
     while (true)
     {

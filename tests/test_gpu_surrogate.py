@@ -248,9 +248,10 @@ def test_render_with_every_pixel_on_rk4_equals_plain_frame(cuda, derive, stride)
         net.close()
 
 
-@pytest.mark.parametrize("w,h,stride,min_interp", [(960, 540, 4, 0.5), (960, 540, 8, 0.5),
-                                                   (333, 197, 8, 0.2)])   # ragged: tiles padded
-def test_anchored_frame_within_one_lsb_of_plain(cuda, derive, w, h, stride, min_interp):
+@pytest.mark.parametrize("w,h,stride,min_interp,scene", [(960, 540, 4, 0.5, "kn"), (960, 540, 8, 0.5, "kn"),
+                                                         (1003, 565, 8, 0.4, "kn"),   # ragged: tiles padded
+                                                         (1920, 1080, 8, 0.5, "kerr")])
+def test_anchored_frame_within_one_lsb_of_plain(cuda, derive, w, h, stride, min_interp, scene):
     """Anchored form without the network gate: RK4 anchors every `stride` pixels,
     the rest interpolated (or black inside the shadow) where the error bound and
     the sky allow.  Most pixels are not traced, the frame is within +-1 LSB of the
@@ -259,7 +260,8 @@ def test_anchored_frame_within_one_lsb_of_plain(cuda, derive, w, h, stride, min_
     net = Net(5)
     try:
         _anchors(net, stride, use_net=0)
-        P = _kn_scene(derive, w, h, az=75.0)
+        # the 4K Kerr-Newman orbit scene, or frame 3 of the 1080p Kerr a* = 0.9 scene
+        P = _kn_scene(derive, w, h, az=75.0) if scene == "kn" else scenes.kerr_pair_1080(derive, w, h)[3]
         out, acc, st = _render(net, P)
         pout, pacc = _plain(P)
         n = w * h
