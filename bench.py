@@ -500,6 +500,7 @@ def surrogate_leg():
             res[gname] = {"gate": {"anchor_stride": gg[0], "network_cell_gate": bool(gg[1]), "min_prob": g[0],
                                    "min_conf": g[1], "crit_band": g[2], "held_stride": g[3]},
                           "interpolated_frac": float(st[7]) / (SG_W * SG_H),
+                          "sky_sampled_frac": float(st[11]) / (SG_W * SG_H),
                           "frame_ms": float(np.median(sur_ms)),
                           "px_within_1lsb": float(np.min(within)),
                           "rk4_pixel_frac": float(np.mean(rk4)),

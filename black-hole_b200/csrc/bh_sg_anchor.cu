@@ -19,7 +19,10 @@
 //     direction and at four directions sqrt(2) bound away differ by less
 //     than maxStep; and the pixel stays below the bloom bright-pass
 //     threshold, so neither its byte nor its neighbours' bloom can move by
-//     a whole step;
+//     a whole step.  The sampled test costs four more sky evaluations and
+//     is needed by a minority of pixels scattered over the sky, so the
+//     resolve pass defers those pixels to a compact buffer and a second
+//     pass (sky_sample_kernel) runs the test on full warps;
 //   * a pixel whose 16 surrounding anchors were all captured without touching
 //     the disk (the inside of the shadow), and whose cell centre the network
 //     (when it gates) also calls captured, is black, as a captured sample is;
@@ -29,6 +32,8 @@
 // (renderSampleHDR, trace.cuh:908-926).
 // No counterpart in the reference.
 // ---------------------------------------------------------------------------
+#include <algorithm>
+
 #include "bh_integrate.cuh"
 #include "bh_post.cuh"
 #include "bh_sg_infer.h"
@@ -119,6 +124,54 @@ __device__ __forceinline__ void push_tile(unsigned* list, unsigned* count, unsig
     list[base + lane] = want ? pix : BH_PIX_SKIP;
 }
 
+// Warp-wide claim of one slot per lane that wants one (all lanes call it): the
+// lanes' slots are consecutive, in lane order, from one atomicAdd on `count`.
+__device__ __forceinline__ unsigned warp_claim(unsigned* count, bool want)
+{
+    const unsigned lane = threadIdx.x & 31u;
+    const unsigned m = __ballot_sync(0xffffffffu, want);
+    if (!m) return 0u;
+    const unsigned leader = (unsigned)__ffs(m) - 1u;
+    unsigned base = 0;
+    if (lane == leader) base = atomicAdd(count, (unsigned)__popc(m));
+    base = __shfl_sync(0xffffffffu, base, leader);
+    return base + (unsigned)__popc(m & ((1u << lane) - 1u));
+}
+
+// The held-out sample of the interpolated pixels: one in `stride`, hashed per frame.
+__device__ __forceinline__ bool held_pick(unsigned pix, unsigned seed, int stride)
+{
+    if (stride <= 0) return false;
+    unsigned h = pix * 0x9E3779B1u ^ (seed * 0x85EBCA77u);
+    h ^= h >> 15; h *= 0x2C1B3C6Du; h ^= h >> 12;
+    return (h % (unsigned)stride) == 0u;
+}
+
+// Records a held-out pixel and its interpolated HDR (all lanes call it); the
+// pixel is traced after the RK4 list and compared (sg_held_compare).
+__device__ __forceinline__ void push_held(const SgAnchorFrame& F, unsigned pix, f3 hdr, bool held)
+{
+    const unsigned k = warp_claim(F.heldCount, held);
+    if (held && k < F.heldCap)
+    {
+        F.heldPix[k] = pix;
+        F.heldPred[k] = make_float4(hdr.x, hdr.y, hdr.z, 1.f);
+    }
+}
+
+// Per-frame tallies (all lanes call it): interpolated pixels, and the
+// rejection reason (1..3) of the traced ones.
+__device__ __forceinline__ void tally(unsigned* stats, bool resolved, int reason)
+{
+    const unsigned lane = threadIdx.x & 31u;
+#pragma unroll
+    for (int k = 0; k < 4; ++k)
+    {
+        const unsigned m = __ballot_sync(0xffffffffu, k == 0 ? resolved : reason == k);
+        if (lane == 0 && m) atomicAdd(stats + k, (unsigned)__popc(m));
+    }
+}
+
 // anchors a 32 x 8 pixel block can reach: columns x0/S - 1 .. (x0+31)/S + 2, rows
 // y0/S - 1 .. (y0+7)/S + 2 (at most 19 x 8 for S >= 2)
 constexpr int kAncCols = 19, kAncRows = 8;
@@ -152,9 +205,10 @@ __global__ void __launch_bounds__(256) anchor_resolve_kernel(const __grid_consta
     }
     __syncthreads();
 
-    bool anchor = false, resolved = false;
+    bool anchor = false, resolved = false, defer = false;
     f3 hdr = v3(0.f, 0.f, 0.f);
-    int reason = 0;                   // 1 anchors / cell gate, 2 error bound, 3 sky sensitivity
+    float4 dir = make_float4(0.f, 0.f, 0.f, 0.f);
+    int reason = 0;                   // 1 anchors / cell gate, 2 error bound, 3 sky sensitivity, 4 deferred
     if (inFrame)
     {
         const int cx = x / S, cy = y / S;
@@ -220,34 +274,22 @@ __global__ void __launch_bounds__(256) anchor_resolve_kernel(const __grid_consta
                 if (eps <= F.epsMax)
                 {
                     const f3 c0 = sky_color(bc, P.gCam);
-                    const f3 y0 = display_value(c0, P.exposure);
-                    bool flat = lum_exposed(c0, P.exposure) < kLumBloomSafe;
-                    // no star within reach: flat without sampling (the common case)
-                    const bool clear = flat && stars_clear(normalize_x(bc), eps);
-                    // two unit vectors orthogonal to the direction
-                    const f3 ref = fabsf(bc.y) < 0.9f ? v3(0.f, 1.f, 0.f) : v3(1.f, 0.f, 0.f);
-                    const f3 u = unit3(v3(ref.y * bc.z - ref.z * bc.y, ref.z * bc.x - ref.x * bc.z,
-                                          ref.x * bc.y - ref.y * bc.x));
-                    const f3 v = v3(bc.y * u.z - bc.z * u.y, bc.z * u.x - bc.x * u.z, bc.x * u.y - bc.y * u.x);
-                    const float r = 1.41421356f * eps;
-#pragma unroll 1
-                    for (int k = 0; k < 4 && flat && !clear; ++k)
-                    {
-                        const float su = (k == 0) ? r : (k == 1 ? -r : 0.f);
-                        const float sv = (k == 2) ? r : (k == 3 ? -r : 0.f);
-                        const f3 dk = unit3(v3(bc.x + su * u.x + sv * v.x, bc.y + su * u.y + sv * v.y,
-                                               bc.z + su * u.z + sv * v.z));
-                        const f3 ck = sky_color(dk, P.gCam);
-                        const f3 yk = display_value(ck, P.exposure);
-                        flat = lum_exposed(ck, P.exposure) < kLumBloomSafe && fabsf(yk.x - y0.x) < F.maxStep &&
-                               fabsf(yk.y - y0.y) < F.maxStep && fabsf(yk.z - y0.z) < F.maxStep;
-                    }
                     reason = 3;
-                    if (flat && isfinite(c0.x) && isfinite(c0.y) && isfinite(c0.z))
+                    if (lum_exposed(c0, P.exposure) < kLumBloomSafe && isfinite(c0.x) && isfinite(c0.y) &&
+                        isfinite(c0.z))
                     {
-                        hdr = c0;
-                        resolved = true;
-                        reason = 0;
+                        if (stars_clear(normalize_x(bc), eps))
+                        {   // no star within reach: flat without sampling (the common case)
+                            hdr = c0;
+                            resolved = true;
+                            reason = 0;
+                        }
+                        else
+                        {
+                            defer = true;
+                            dir = make_float4(bc.x, bc.y, bc.z, eps);
+                            reason = 4;
+                        }
                     }
                 }
             }
@@ -256,39 +298,72 @@ __global__ void __launch_bounds__(256) anchor_resolve_kernel(const __grid_consta
     }
     if (anchor || resolved) acc[pix] = make_float4(hdr.x, hdr.y, hdr.z, 1.f);
 
-    // held-out sample of the interpolated pixels (hashed per frame), also traced and compared
-    bool held = false;
-    if (resolved && F.heldStride > 0)
+    // deferred pixels to the sample buffer; beyond its capacity they are traced
+    const unsigned k = warp_claim(F.sampleCount, defer);
+    if (defer && k < F.sampleCap)
     {
-        unsigned h = pix * 0x9E3779B1u ^ (F.frameSeed * 0x85EBCA77u);
-        h ^= h >> 15; h *= 0x2C1B3C6Du; h ^= h >> 12;
-        held = (h % (unsigned)F.heldStride) == 0u;
+        F.sampleDir[k] = dir;
+        F.samplePix[k] = pix;
     }
-    const bool trace = inFrame && !anchor && !resolved;
+    else if (defer) reason = 3;
+    const bool trace = inFrame && !anchor && !resolved && reason != 4;
     push_tile(F.list, F.listCount, F.stats + 4, pix, trace);   // held-out pixels: traced from heldPix
-    const unsigned mh = __ballot_sync(0xffffffffu, held);
-    if (mh)
+    push_held(F, pix, hdr, resolved && held_pick(pix, F.frameSeed, F.heldStride));
+    tally(F.stats, inFrame && !anchor && resolved, inFrame && !anchor ? reason : 0);
+}
+
+// Second pass over the deferred pixels: the sampled flatness test, one pixel per
+// thread.  A flat pixel is written as in the resolve pass; the others are
+// appended to the RK4 list one by one (after the resolve pass's whole tiles).
+__global__ void __launch_bounds__(256) sky_sample_kernel(const __grid_constant__ SgAnchorFrame F)
+{
+    const TraceParams& P = F.tp;
+    const unsigned n = min(*F.sampleCount, F.sampleCap);
+    float4* acc = reinterpret_cast<float4*>(P.out);
+    const unsigned lane = threadIdx.x & 31u;
+    for (unsigned base = blockIdx.x * blockDim.x; base < n; base += gridDim.x * blockDim.x)
     {
-        unsigned base = 0;
-        if (lane == __ffs(mh) - 1) base = atomicAdd(F.heldCount, (unsigned)__popc(mh));
-        base = __shfl_sync(0xffffffffu, base, __ffs(mh) - 1);
-        if (held)
+        const unsigned k = base + threadIdx.x;
+        const bool valid = k < n;
+        bool flat = false;
+        f3 c0 = v3(0.f, 0.f, 0.f);
+        unsigned pix = 0;
+        if (valid)
         {
-            const unsigned k = base + __popc(mh & ((1u << lane) - 1u));
-            if (k < F.heldCap)
+            const float4 e = F.sampleDir[k];
+            pix = F.samplePix[k];
+            const f3 bc = v3(e.x, e.y, e.z);
+            const float eps = e.w;
+            c0 = sky_color(bc, P.gCam);
+            const f3 y0 = display_value(c0, P.exposure);
+            // two unit vectors orthogonal to the direction
+            const f3 ref = fabsf(bc.y) < 0.9f ? v3(0.f, 1.f, 0.f) : v3(1.f, 0.f, 0.f);
+            const f3 u = unit3(v3(ref.y * bc.z - ref.z * bc.y, ref.z * bc.x - ref.x * bc.z,
+                                  ref.x * bc.y - ref.y * bc.x));
+            const f3 v = v3(bc.y * u.z - bc.z * u.y, bc.z * u.x - bc.x * u.z, bc.x * u.y - bc.y * u.x);
+            const float r = 1.41421356f * eps;
+            flat = true;
+#pragma unroll 1
+            for (int j = 0; j < 4 && flat; ++j)
             {
-                F.heldPix[k] = pix;
-                F.heldPred[k] = make_float4(hdr.x, hdr.y, hdr.z, 1.f);
+                const float su = (j == 0) ? r : (j == 1 ? -r : 0.f);
+                const float sv = (j == 2) ? r : (j == 3 ? -r : 0.f);
+                const f3 dk = unit3(v3(bc.x + su * u.x + sv * v.x, bc.y + su * u.y + sv * v.y,
+                                       bc.z + su * u.z + sv * v.z));
+                const f3 ck = sky_color(dk, P.gCam);
+                const f3 yk = display_value(ck, P.exposure);
+                flat = lum_exposed(ck, P.exposure) < kLumBloomSafe && fabsf(yk.x - y0.x) < F.maxStep &&
+                       fabsf(yk.y - y0.y) < F.maxStep && fabsf(yk.z - y0.z) < F.maxStep;
             }
+            if (flat) acc[pix] = make_float4(c0.x, c0.y, c0.z, 1.f);
         }
-    }
-    // per-frame tallies: interpolated pixels and the rejection reason of the others
-#pragma unroll
-    for (int k = 0; k < 4; ++k)
-    {
-        const bool mine = inFrame && !anchor && (k == 0 ? resolved : reason == k);
-        const unsigned m = __ballot_sync(0xffffffffu, mine);
-        if (lane == 0 && m) atomicAdd(F.stats + k, (unsigned)__popc(m));
+        const bool trace = valid && !flat;
+        const unsigned m = __ballot_sync(0xffffffffu, trace);
+        const unsigned slot = warp_claim(F.listCount, trace);
+        if (trace) F.list[slot] = pix;
+        if (lane == 0 && m) atomicAdd(F.stats + 4, (unsigned)__popc(m));
+        push_held(F, pix, c0, flat && held_pick(pix, F.frameSeed, F.heldStride));
+        tally(F.stats, flat, trace ? 3 : 0);
     }
 }
 
@@ -300,5 +375,11 @@ cudaError_t sg_anchor_resolve(const SgAnchorFrame& F, cudaStream_t s)
     if (F.S < 2 || F.nx < 1 || F.ny < 1) return cudaErrorInvalidValue;
     dim3 grid((P.W + 31) / 32, (P.H + 7) / 8);
     anchor_resolve_kernel<<<grid, 256, 0, s>>>(F);
+    cudaError_t e = cudaGetLastError();
+    if (e != cudaSuccess || F.sampleCap == 0) return e;
+    int dev = 0, sms = 148;
+    if (cudaGetDevice(&dev) == cudaSuccess) cudaDeviceGetAttribute(&sms, cudaDevAttrMultiProcessorCount, dev);
+    const unsigned blocks = std::min((F.sampleCap + 255u) / 256u, (unsigned)sms * 8u);
+    sky_sample_kernel<<<blocks, 256, 0, s>>>(F);
     return cudaGetLastError();
 }

@@ -105,10 +105,14 @@ struct BHSurrogate
     unsigned* list = nullptr;
     size_t listCap = 0;
     unsigned* counters = nullptr;     // [0] RK4 list groups x 32, [1] held-out count, [4..7] held-out statistics,
-                                      // [8..11] anchored tallies, [12] listed pixels, [13] list + held-out length
+                                      // [8..11] anchored tallies, [12] listed pixels, [13] list + held-out length,
+                                      // [14] pixels deferred to the sampled sky test
     unsigned* heldPix = nullptr;
     float4* heldPred = nullptr;
     unsigned heldCap = 0;
+    float4* sampleDir = nullptr;      // anchored form: pixels deferred to the sampled sky test
+    unsigned* samplePix = nullptr;
+    unsigned sampleCap = 0;
     unsigned frames = 0;
     // acceptance gate of the surrogate frame
     float minProb = 0.95f, minConf = 0.95f, critBand = 0.02f;
@@ -144,7 +148,7 @@ void freeAll(BHSurrogate* s)
     sg_free_batch(S);
     void* ps[] = {S.params, S.grads, S.adamM, S.adamV, S.W, S.Wt, S.biasPacked, S.loss, S.dsIn, S.dsTgt, s->list,
                   s->counters, s->heldPix, s->heldPred, s->bIn, s->bTgt, s->anchorPix, s->anchorSlot, s->anchorRec,
-                  s->cellPix, s->cellGate};
+                  s->cellPix, s->cellGate, s->sampleDir, s->samplePix};
     for (void* p : ps)
         if (p) cudaFree(p);
     if (s->stream) cudaStreamDestroy(s->stream);
@@ -212,27 +216,34 @@ cudaError_t criticalCurve(BHSurrogate* s, const RenderParams& P0, float* crit)
 
 // Frame scratch of a W x H frame.  The RK4 list holds whole 32-entry groups
 // (8x4 tiles in the anchored form, 32 consecutive pixels in the network form),
-// bounded by the frame padded to whole tiles or whole groups, followed by the
+// bounded by the frame padded to whole tiles or whole groups; then, in the
+// anchored form, the deferred pixels the sampled sky test rejects (at most
+// sampleCap, a quarter of the frame: more are traced in their tiles); then the
 // held-out sample (at most heldCap pixels).
 cudaError_t ensureFrame(BHSurrogate* s, int W, int H)
 {
     const size_t pixels = (size_t)W * H;
     const size_t stride = s->heldStride > 0 ? (size_t)s->heldStride : pixels + 1;
     const size_t want = std::min(pixels, pixels / stride * 2 + 4096);
+    const size_t sampleCap = std::min(pixels, pixels / 4 + 4096);
     const size_t listLen =
-        std::max((size_t)((W + 7) / 8 * 8) * (size_t)((H + 3) / 4 * 4), (pixels + 31) / 32 * 32) + want;
-    if (listLen <= s->listCap && want <= s->heldCap) return cudaSuccess;
-    if (s->list) cudaFree(s->list);
-    if (s->heldPix) cudaFree(s->heldPix);
-    if (s->heldPred) cudaFree(s->heldPred);
-    s->list = nullptr; s->heldPix = nullptr; s->heldPred = nullptr; s->listCap = 0; s->heldCap = 0;
+        std::max((size_t)((W + 7) / 8 * 8) * (size_t)((H + 3) / 4 * 4), (pixels + 31) / 32 * 32) + sampleCap + want;
+    if (listLen <= s->listCap && want <= s->heldCap && sampleCap <= s->sampleCap) return cudaSuccess;
+    void* old[] = {s->list, s->heldPix, s->heldPred, s->sampleDir, s->samplePix};
+    for (void* p : old)
+        if (p) cudaFree(p);
+    s->list = nullptr; s->heldPix = nullptr; s->heldPred = nullptr; s->sampleDir = nullptr; s->samplePix = nullptr;
+    s->listCap = 0; s->heldCap = 0; s->sampleCap = 0;
     const unsigned cap = (unsigned)want;
     cudaError_t e = bh_device_alloc(reinterpret_cast<void**>(&s->list), listLen * sizeof(unsigned));
     if (e == cudaSuccess) e = bh_device_alloc(reinterpret_cast<void**>(&s->heldPix), cap * sizeof(unsigned));
     if (e == cudaSuccess) e = bh_device_alloc(reinterpret_cast<void**>(&s->heldPred), cap * sizeof(float4));
+    if (e == cudaSuccess) e = bh_device_alloc(reinterpret_cast<void**>(&s->sampleDir), sampleCap * sizeof(float4));
+    if (e == cudaSuccess) e = bh_device_alloc(reinterpret_cast<void**>(&s->samplePix), sampleCap * sizeof(unsigned));
     if (e != cudaSuccess) return e;
     s->listCap = listLen;
     s->heldCap = cap;
+    s->sampleCap = (unsigned)sampleCap;
     return cudaSuccess;
 }
 
@@ -340,6 +351,10 @@ cudaError_t anchoredFrame(BHSurrogate* s, const RenderParams& P, float4* accum, 
     A.heldCap = s->heldCap;
     A.heldStride = s->heldStride;
     A.frameSeed = ++s->frames;
+    A.sampleDir = s->sampleDir;
+    A.samplePix = s->samplePix;
+    A.sampleCount = s->counters + 14;
+    A.sampleCap = s->sampleCap;
     A.stats = s->counters + 8;      // [8..11] tallies, [12] pixels on the list
     s->lastAnchors = nA;
     return sg_anchor_resolve(A, stream);
@@ -662,6 +677,7 @@ cudaError_t bhSurrogateFrameStats(BHSurrogate* s, BHSurrogateStats* st)
     st->rejectAnchors = c[9];
     st->rejectBound = c[10];
     st->rejectSky = c[11];
+    st->skySampled = s->lastAnchors ? std::min(c[14], s->sampleCap) : 0u;
     return cudaSuccess;
 }
 

@@ -55,7 +55,10 @@ cudaError_t sg_infer_launch(const SgInferArgs& a, const SgFrame* frame, cudaStre
 // by RK4 into `anchors` (BH_OUT_ANCHOR records, in trace order).  The resolve
 // pass writes every anchor's HDR and every pixel it can interpolate to the
 // accumulation buffer (tp.out), appends the pixels to trace to `list` in
-// whole 8x4 tiles, and records the held-out sample in heldPix.
+// whole 8x4 tiles, and records the held-out sample in heldPix.  Pixels whose
+// sky needs the sampled flatness test (a star may lie within reach of the
+// bound) are deferred to a compact buffer and tested by a second pass with
+// full warps, which resolves them or appends them to the list one by one.
 struct SgAnchorFrame
 {
     TraceParams tp;
@@ -74,6 +77,10 @@ struct SgAnchorFrame
     unsigned heldCap;
     int heldStride;
     unsigned frameSeed;
+    float4* sampleDir;              // deferred pixels: (interpolated direction, error bound)
+    unsigned* samplePix;
+    unsigned* sampleCount;          // deferred pixels claimed (beyond sampleCap: traced instead)
+    unsigned sampleCap;
     unsigned* stats;                // [0] interpolated, [1] rejected by the anchors / cell gate,
                                     // [2] by the error bound, [3] by the sky sensitivity,
                                     // [4] pixels on the list (the list itself is padded to tiles;

@@ -167,6 +167,7 @@ typedef struct BHSurrogateStats
     unsigned rejectAnchors;   /* traced: an anchor not sky-only, or the cell gate, or the frame border */
     unsigned rejectBound;     /* traced: interpolation error bound above epsMax */
     unsigned rejectSky;       /* traced: sky not flat within the bound */
+    unsigned skySampled;      /* anchored form: pixels whose sky flatness needed the sampled test */
 } BHSurrogateStats;
 cudaError_t bhSurrogateFrameStats(BHSurrogate* s, BHSurrogateStats* stats);
 

@@ -273,6 +273,7 @@ def test_anchored_frame_within_one_lsb_of_plain(cuda, derive, w, h, stride, min_
         assert st[7] > min_interp * n                                 # interpolated (or shadow)
         assert st[7] + st[8] + st[9] + st[10] + anchors == n           # every pixel accounted for once
         assert st[1] == n - st[7] + st[2]                              # traced: the rest + held-out
+        assert 0 < st[11] <= st[7] + st[10]        # sampled sky test: interpolated or rejected by the sky
         assert float((d <= 1).mean()) >= 0.999
         assert st[3] <= max(2, st[2] // 100)                           # held-out sample over 1 LSB
     finally:
