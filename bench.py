@@ -492,7 +492,7 @@ def surrogate_leg():
                 sur_ms.append(timed(lambda: sur(P)))
                 d = (fa.out[..., :3].int() - fb.out[..., :3].int()).abs().amax(dim=-1)
                 within.append(float((d <= 1).float().mean()))
-                st = np.zeros(12, dtype=np.uint32)
+                st = np.zeros(16, dtype=np.uint32)
                 lib.check(L.bhSurrogateFrameStats(h, st.ctypes.data_as(C.c_void_p)), "stats")
                 rk4.append(float(st[1]) / (SG_W * SG_H))
                 held += int(st[2])

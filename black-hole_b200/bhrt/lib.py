@@ -63,6 +63,7 @@ _SIGNATURES = {
     "bhSurrogateFrameStats": (_int, [_vp, _vp]),
     "bhSurrogateSetGate": (_int, [_vp, C.c_float, C.c_float, C.c_float, _int]),
     "bhSurrogateSetAnchors": (_int, [_vp, _int, _int, C.c_float, C.c_float]),
+    "bhSurrogateSetAnchorSteps": (_int, [_vp, _int]),
     "bhVersion": (C.c_char_p, []),
 }
 

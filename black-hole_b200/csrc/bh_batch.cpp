@@ -52,6 +52,8 @@ cudaError_t makePlan(const BHView* views, int n, Plan& pl, bool keepOrder)
         bhSanitizeRenderParams(&pl.params[i]);
         cudaError_t e = checkView(views[i], pl.params[i]);
         if (e != cudaSuccess) return e;
+        if ((size_t)pl.params[i].width * (size_t)pl.params[i].height > (size_t)BH_MAX_RAYS)
+            return cudaErrorInvalidValue;
     }
     if (!keepOrder)
     {

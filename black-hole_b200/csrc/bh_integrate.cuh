@@ -48,9 +48,13 @@ constexpr float kPolarCap = 1.0f / 64.0f;
 // A finished ray as it waits for shading: outcome flags, the radiance gathered
 // from the disk, and the six state values from which the escape direction is
 // rebuilt at shading time (so the finishing lane only stores, and the
-// trigonometry runs later with the whole warp converged).
-constexpr unsigned kRayHorizon = 1u << 31, kRayEscaped = 1u << 30, kRayUseState = 1u << 29;
-constexpr unsigned kRayKeyMask = kRayUseState - 1u;
+// trigonometry runs later with the whole warp converged).  The key holds the
+// ray's pixel (or list position) in its low 28 bits and four flags above:
+// captured, escaped, escape direction from the state, step budget spent.
+constexpr unsigned kRayHorizon = 1u << 31, kRayEscaped = 1u << 30, kRayUseState = 1u << 29,
+                   kRayExhausted = 1u << 28;
+constexpr unsigned kRayKeyMask = kRayExhausted - 1u;
+static_assert(kRayKeyMask + 1u == BH_MAX_RAYS, "ray key width");
 
 template <class R>
 struct PackedRay
@@ -374,7 +378,8 @@ struct SphRay
     BH_DEV void pack(const TraceParams& P, unsigned key, PackedRay<R>& q, PackedStats* st) const
     {
         const bool useState = escaped && haveDir;
-        q.key = key | (horizon ? kRayHorizon : 0u) | (escaped ? kRayEscaped : 0u) | (useState ? kRayUseState : 0u);
+        q.key = key | (horizon ? kRayHorizon : 0u) | (escaped ? kRayEscaped : 0u) | (useState ? kRayUseState : 0u) |
+                (step >= P.maxSteps ? kRayExhausted : 0u);
         q.acc[0] = accum.x; q.acc[1] = accum.y; q.acc[2] = accum.z;
         q.trans = trans;
         q.f[0] = ud; q.f[1] = dud; q.f[2] = phid; q.f[3] = e2x; q.f[4] = e2y; q.f[5] = e2z;
@@ -820,7 +825,8 @@ struct KerrRay
     BH_DEV void pack(const TraceParams& P, unsigned key, PackedRay<R>& q, PackedStats* st) const
     {
         const bool useState = escaped && useDeriv;
-        q.key = key | (horizon ? kRayHorizon : 0u) | (escaped ? kRayEscaped : 0u) | (useState ? kRayUseState : 0u);
+        q.key = key | (horizon ? kRayHorizon : 0u) | (escaped ? kRayEscaped : 0u) | (useState ? kRayUseState : 0u) |
+                (step >= P.maxSteps ? kRayExhausted : 0u);
         q.acc[0] = accum.x; q.acc[1] = accum.y; q.acc[2] = accum.z;
         q.trans = trans;
         q.f[0] = r; q.f[1] = th; q.f[2] = ph;

@@ -23,6 +23,10 @@
 //     is needed by a minority of pixels scattered over the sky, so the
 //     resolve pass defers those pixels to a compact buffer and a second
 //     pass (sky_sample_kernel) runs the test on full warps;
+//   * the anchors are traced with a step budget that may be below the frame's
+//     maxSteps (the few rays that graze the photon sphere set the anchor
+//     pass's duration); an anchor that spends it is traced in full on the
+//     list, and no pixel interpolates from it;
 //   * a pixel whose 16 surrounding anchors were all captured without touching
 //     the disk (the inside of the shadow), and whose cell centre the network
 //     (when it gates) also calls captured, is black, as a captured sample is;
@@ -185,12 +189,17 @@ __global__ void __launch_bounds__(256) anchor_resolve_kernel(const __grid_consta
     __shared__ float4 sAnc[kAncRows][kAncCols];
     const TraceParams& P = F.tp;
     const int warp = threadIdx.x >> 5, lane = threadIdx.x & 31;
-    const int x = blockIdx.x * 32 + (warp & 3) * 8 + (lane & 7), y = blockIdx.y * 8 + (warp >> 2) * 4 + (lane >> 3);
+    // blocks run nearest the screen centre first, so the list's first tiles hold the
+    // long rays around the shadow and the tracer does not end on them
+    const unsigned blk = F.blockOrder ? __ldg(F.blockOrder + blockIdx.x) : blockIdx.x;
+    const unsigned bxs = (unsigned)(P.W + 31) / 32u;
+    const int bx = (int)(blk % bxs), by = (int)(blk / bxs);
+    const int x = bx * 32 + (warp & 3) * 8 + (lane & 7), y = by * 8 + (warp >> 2) * 4 + (lane >> 3);
     const bool inFrame = x < P.W && y < P.H;
     const int S = F.S;
     const unsigned pix = inFrame ? (unsigned)y * (unsigned)P.W + (unsigned)x : 0u;
     float4* acc = reinterpret_cast<float4*>(P.out);
-    const int ax0 = (int)(blockIdx.x * 32) / S - 1, ay0 = (int)(blockIdx.y * 8) / S - 1;
+    const int ax0 = (bx * 32) / S - 1, ay0 = (by * 8) / S - 1;
     for (int i = threadIdx.x; i < kAncRows * kAncCols; i += blockDim.x)
     {
         const int r = i / kAncCols, c = i - r * kAncCols;
@@ -205,7 +214,7 @@ __global__ void __launch_bounds__(256) anchor_resolve_kernel(const __grid_consta
     }
     __syncthreads();
 
-    bool anchor = false, resolved = false, defer = false;
+    bool anchor = false, resolved = false, defer = false, incomplete = false;
     f3 hdr = v3(0.f, 0.f, 0.f);
     float4 dir = make_float4(0.f, 0.f, 0.f, 0.f);
     int reason = 0;                   // 1 anchors / cell gate, 2 error bound, 3 sky sensitivity, 4 deferred
@@ -213,10 +222,12 @@ __global__ void __launch_bounds__(256) anchor_resolve_kernel(const __grid_consta
     {
         const int cx = x / S, cy = y / S;
         if (x == cx * S && y == cy * S)
-        {   // an anchor: its own RK4 sample
+        {   // an anchor: its own RK4 sample, unless the anchor pass's step budget ran out
             const BHAnchor& a = F.anchors[F.slot[cy * F.nx + cx]];
             hdr = v3(a.hdr.x, a.hdr.y, a.hdr.z);
-            anchor = true;
+            incomplete = (a.flags & BH_ANCHOR_INCOMPLETE) != 0u;
+            anchor = !incomplete;
+            reason = incomplete ? 1 : 0;
         }
         else if (cx >= 1 && cy >= 1 && cx + 2 < F.nx && cy + 2 < F.ny)
         {
@@ -310,6 +321,8 @@ __global__ void __launch_bounds__(256) anchor_resolve_kernel(const __grid_consta
     push_tile(F.list, F.listCount, F.stats + 4, pix, trace);   // held-out pixels: traced from heldPix
     push_held(F, pix, hdr, resolved && held_pick(pix, F.frameSeed, F.heldStride));
     tally(F.stats, inFrame && !anchor && resolved, inFrame && !anchor ? reason : 0);
+    const unsigned mi = __ballot_sync(0xffffffffu, incomplete);
+    if (lane == 0 && mi) atomicAdd(F.stats + 7, (unsigned)__popc(mi));
 }
 
 // Second pass over the deferred pixels: the sampled flatness test, one pixel per
@@ -373,13 +386,13 @@ cudaError_t sg_anchor_resolve(const SgAnchorFrame& F, cudaStream_t s)
 {
     const TraceParams& P = F.tp;
     if (F.S < 2 || F.nx < 1 || F.ny < 1) return cudaErrorInvalidValue;
-    dim3 grid((P.W + 31) / 32, (P.H + 7) / 8);
-    anchor_resolve_kernel<<<grid, 256, 0, s>>>(F);
+    const unsigned blocks = (unsigned)((P.W + 31) / 32) * (unsigned)((P.H + 7) / 8);
+    anchor_resolve_kernel<<<blocks, 256, 0, s>>>(F);
     cudaError_t e = cudaGetLastError();
     if (e != cudaSuccess || F.sampleCap == 0) return e;
     int dev = 0, sms = 148;
     if (cudaGetDevice(&dev) == cudaSuccess) cudaDeviceGetAttribute(&sms, cudaDevAttrMultiProcessorCount, dev);
-    const unsigned blocks = std::min((F.sampleCap + 255u) / 256u, (unsigned)sms * 8u);
-    sky_sample_kernel<<<blocks, 256, 0, s>>>(F);
+    const unsigned sBlocks = std::min((F.sampleCap + 255u) / 256u, (unsigned)sms * 8u);
+    sky_sample_kernel<<<sBlocks, 256, 0, s>>>(F);
     return cudaGetLastError();
 }

@@ -27,6 +27,7 @@ constexpr int kHidW = 256 * 256;           // one hidden weight matrix
 constexpr int kWCount = 4 * kHidW + 256 * 64;
 constexpr int kBiasCount = 4 * 256 + 16;
 constexpr int kHeldStride = 256;
+constexpr int kAnchorSteps = 600;
 constexpr float kPi = 3.14159265358979f;
 
 // uniform float in [lo, hi) from a 32-bit generator (portable, unlike std distributions)
@@ -106,7 +107,7 @@ struct BHSurrogate
     size_t listCap = 0;
     unsigned* counters = nullptr;     // [0] RK4 list groups x 32, [1] held-out count, [4..7] held-out statistics,
                                       // [8..11] anchored tallies, [12] listed pixels, [13] list + held-out length,
-                                      // [14] pixels deferred to the sampled sky test
+                                      // [14] pixels deferred to the sampled sky test, [15] incomplete anchors
     unsigned* heldPix = nullptr;
     float4* heldPred = nullptr;
     unsigned heldCap = 0;
@@ -129,10 +130,13 @@ struct BHSurrogate
     // anchored frames: RK4 anchors every anchorStride pixels (0: the network's own directions)
     int anchorStride = 8;
     bool anchorNet = true;
+    int anchorSteps = kAnchorSteps;   // step budget of the anchor pass (0: the frame's maxSteps)
     float epsMax = 1e-4f, maxStep = 0.5f;
     int aW = 0, aH = 0, aS = 0, aNx = 0, aNy = 0;
     unsigned* anchorPix = nullptr;    // anchor pixels in trace order
     unsigned* anchorSlot = nullptr;   // anchor (ax, ay) -> its index in anchorPix / anchorRec
+    unsigned* blockOrder = nullptr;   // resolve pass: 32 x 8 pixel blocks, nearest the screen centre first
+    size_t bCapOrder = 0;
     BHAnchor* anchorRec = nullptr;
     unsigned* cellPix = nullptr;      // cell-centre pixels
     float2* cellGate = nullptr;
@@ -148,7 +152,7 @@ void freeAll(BHSurrogate* s)
     sg_free_batch(S);
     void* ps[] = {S.params, S.grads, S.adamM, S.adamV, S.W, S.Wt, S.biasPacked, S.loss, S.dsIn, S.dsTgt, s->list,
                   s->counters, s->heldPix, s->heldPred, s->bIn, s->bTgt, s->anchorPix, s->anchorSlot, s->anchorRec,
-                  s->cellPix, s->cellGate, s->sampleDir, s->samplePix};
+                  s->cellPix, s->cellGate, s->sampleDir, s->samplePix, s->blockOrder};
     for (void* p : ps)
         if (p) cudaFree(p);
     if (s->stream) cudaStreamDestroy(s->stream);
@@ -304,6 +308,26 @@ cudaError_t ensureAnchors(BHSurrogate* s, int W, int H, int S)
             c[(size_t)y * (nx - 1) + x] = (unsigned)(y * S + S / 2) * (unsigned)W + (unsigned)(x * S + S / 2);
     if ((e = cudaMemcpy(s->anchorPix, a.data(), nA * sizeof(unsigned), cudaMemcpyHostToDevice))) return e;
     if ((e = cudaMemcpy(s->anchorSlot, slot.data(), nA * sizeof(unsigned), cudaMemcpyHostToDevice))) return e;
+    // resolve blocks (32 x 8 pixels) nearest the screen centre first
+    const int rbx = (W + 31) / 32, rby = (H + 7) / 8;
+    const size_t nB = (size_t)rbx * rby;
+    std::vector<unsigned> blocks(nB);
+    std::vector<float> bkey(nB);
+    for (size_t b = 0; b < nB; ++b)
+    {
+        blocks[b] = (unsigned)b;
+        const float dx = (float)(b % rbx) * 32.f + 16.f - 0.5f * W, dy = (float)(b / rbx) * 8.f + 4.f - 0.5f * H;
+        bkey[b] = dx * dx + dy * dy;
+    }
+    std::stable_sort(blocks.begin(), blocks.end(), [&](unsigned p, unsigned q) { return bkey[p] < bkey[q]; });
+    if (nB > s->bCapOrder)
+    {
+        if (s->blockOrder) cudaFree(s->blockOrder);
+        s->blockOrder = nullptr; s->bCapOrder = 0;
+        if ((e = bh_device_alloc(reinterpret_cast<void**>(&s->blockOrder), nB * sizeof(unsigned)))) return e;
+        s->bCapOrder = nB;
+    }
+    if ((e = cudaMemcpy(s->blockOrder, blocks.data(), nB * sizeof(unsigned), cudaMemcpyHostToDevice))) return e;
     if ((e = cudaMemcpy(s->cellPix, c.data(), nC * sizeof(unsigned), cudaMemcpyHostToDevice))) return e;
     s->aW = W; s->aH = H; s->aS = S; s->aNx = nx; s->aNy = ny;
     return cudaSuccess;
@@ -330,6 +354,7 @@ cudaError_t anchoredFrame(BHSurrogate* s, const RenderParams& P, float4* accum, 
         if ((e = sg_infer_launch(a, &F, stream)) != cudaSuccess) return e;
     }
     TraceParams t = bh_frame_params(P, BH_OUT_ANCHOR, s->anchorRec);
+    if (s->anchorSteps > 0 && s->anchorSteps < t.maxSteps) t.maxSteps = s->anchorSteps;
     t.pixList = s->anchorPix;
     t.nRays = nA;
     if ((e = bh_device_counter(&t.counter)) != cudaSuccess) return e;
@@ -338,6 +363,7 @@ cudaError_t anchoredFrame(BHSurrogate* s, const RenderParams& P, float4* accum, 
     A.tp = bh_frame_params(P, BH_OUT_ACCUM, accum);
     A.anchors = s->anchorRec;
     A.slot = s->anchorSlot;
+    A.blockOrder = s->blockOrder;
     A.S = S; A.nx = s->aNx; A.ny = s->aNy;
     A.cellGate = s->anchorNet ? s->cellGate : nullptr;
     A.minProb = s->minProb;
@@ -678,6 +704,7 @@ cudaError_t bhSurrogateFrameStats(BHSurrogate* s, BHSurrogateStats* st)
     st->rejectBound = c[10];
     st->rejectSky = c[11];
     st->skySampled = s->lastAnchors ? std::min(c[14], s->sampleCap) : 0u;
+    st->anchorsIncomplete = s->lastAnchors ? c[15] : 0u;
     return cudaSuccess;
 }
 
@@ -703,6 +730,13 @@ extern "C" cudaError_t bhSurrogateSetAnchors(BHSurrogate* s, int stride, int use
     s->anchorNet = useNetwork != 0;
     s->epsMax = epsMax;
     s->maxStep = maxStep;
+    return cudaSuccess;
+}
+
+extern "C" cudaError_t bhSurrogateSetAnchorSteps(BHSurrogate* s, int maxSteps)
+{
+    if (!s || maxSteps < 0) return cudaErrorInvalidValue;
+    s->anchorSteps = maxSteps;
     return cudaSuccess;
 }
 

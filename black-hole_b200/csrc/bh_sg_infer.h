@@ -64,6 +64,7 @@ struct SgAnchorFrame
     TraceParams tp;
     const BHAnchor* anchors;        // in trace order (8x4 anchor tiles, centre-out)
     const unsigned* slot;           // anchor (ax, ay) -> its record: slot[ay * nx + ax]
+    const unsigned* blockOrder;     // null, or resolve block k -> 32 x 8 pixel block (row-major index)
     int S, nx, ny;
     const float2* cellGate;         // null, or per cell (nx - 1) x (ny - 1): (P(sky), P(shadow))
     float minProb;                  // cell gate: probability of the cell's class needed at its centre
@@ -84,7 +85,7 @@ struct SgAnchorFrame
     unsigned* stats;                // [0] interpolated, [1] rejected by the anchors / cell gate,
                                     // [2] by the error bound, [3] by the sky sensitivity,
                                     // [4] pixels on the list (the list itself is padded to tiles;
-                                    // held-out pixels are not on it)
+                                    // held-out pixels are not on it), [7] incomplete anchors
 };
 
 cudaError_t sg_anchor_resolve(const SgAnchorFrame& F, cudaStream_t s);

@@ -115,7 +115,8 @@ BH_DEV void shade_slot(const TraceParams& P, const PackedRay<typename Ray::Real>
         BHAnchor a;
         a.escDir = make_float3(esc.x, esc.y, esc.z);
         const bool disk = q.trans < 1.f || q.acc[0] > 0.f || q.acc[1] > 0.f || q.acc[2] > 0.f;
-        a.flags = (escaped ? BH_ANCHOR_ESCAPED : 0u) | (horizon ? BH_ANCHOR_HORIZON : 0u) | (disk ? BH_ANCHOR_DISK : 0u);
+        a.flags = (escaped ? BH_ANCHOR_ESCAPED : 0u) | (horizon ? BH_ANCHOR_HORIZON : 0u) | (disk ? BH_ANCHOR_DISK : 0u) |
+                  ((q.key & kRayExhausted) ? BH_ANCHOR_INCOMPLETE : 0u);
         a.hdr = make_float3(hdr.x, hdr.y, hdr.z);
         a.trans = q.trans;
         reinterpret_cast<BHAnchor*>(P.out)[key] = a;
@@ -398,6 +399,8 @@ cudaError_t launch_one(const TraceParams& P, int blocksPerSm, cudaStream_t strea
 cudaError_t bh_launch_trace(const TraceParams& P, int precision, bool stats, int blocksPerSm,
                             cudaStream_t stream)
 {
+    if (P.nRays > BH_MAX_RAYS || (!P.dirs && (size_t)P.W * (size_t)P.H > (size_t)BH_MAX_RAYS))
+        return cudaErrorInvalidValue;
     cudaError_t e = cudaMemsetAsync(P.counter, 0, sizeof(unsigned), stream);
     if (e != cudaSuccess) return e;
     if (P.nRays == 0) return cudaSuccess;

@@ -28,7 +28,13 @@ struct BHAnchor
     float3 hdr;
     float trans;
 };
-enum { BH_ANCHOR_ESCAPED = 1u, BH_ANCHOR_HORIZON = 2u, BH_ANCHOR_DISK = 4u };
+// BH_ANCHOR_INCOMPLETE: the ray spent the launch's step budget (which, for
+// anchors, may be below the frame's maxSteps): its record is not the pixel's.
+enum { BH_ANCHOR_ESCAPED = 1u, BH_ANCHOR_HORIZON = 2u, BH_ANCHOR_DISK = 4u, BH_ANCHOR_INCOMPLETE = 8u };
+
+// Largest frame (pixels) or ray count of one launch: a ray's key carries its
+// pixel or list position in 28 bits (16384 x 16384 pixels).
+constexpr unsigned BH_MAX_RAYS = 1u << 28;
 
 // pixel-list entry that traces nothing (pads a 32-entry group of a list)
 constexpr unsigned BH_PIX_SKIP = 0xFFFFFFFFu;

@@ -126,7 +126,9 @@ cudaError_t bhSurrogateTrain(BHSurrogate* s, int steps, int batch, float lr, uns
  *    bound (display values within maxStep of a byte step, below the bloom
  *    threshold); a pixel whose 16 anchors were all captured without the disk
  *    (and whose cell centre the network calls captured) is black; every other
- *    pixel is traced;
+ *    pixel is traced.  The anchors are traced with a step budget
+ *    (bhSurrogateSetAnchorSteps); an anchor that spends it is traced in full
+ *    with the rest, and no pixel interpolates from it;
  *  - network (stride 0): the fused kernel resolves the pixels it is sure of
  *    from its own escape direction (escaped or captured without the disk,
  *    class probability and confidence >= 0.95, farther than 2 % from the
@@ -153,6 +155,13 @@ cudaError_t bhSurrogateSetGate(BHSurrogate* s, float minProb, float minConf, flo
  * that bound. */
 cudaError_t bhSurrogateSetAnchors(BHSurrogate* s, int stride, int useNetwork, float epsMax, float maxStep);
 
+/* Step budget of the anchored form's anchor pass (default 600; 0: the frame's
+ * maxSteps).  The pass lasts as long as its longest ray, and the few rays that
+ * graze the photon sphere take several times the median step count; an anchor
+ * that spends the budget is traced again in full with the other RK4 pixels,
+ * so the frame does not depend on it. */
+cudaError_t bhSurrogateSetAnchorSteps(BHSurrogate* s, int maxSteps);
+
 /* Statistics of the last rendered frame (blocking). */
 typedef struct BHSurrogateStats
 {
@@ -168,6 +177,8 @@ typedef struct BHSurrogateStats
     unsigned rejectBound;     /* traced: interpolation error bound above epsMax */
     unsigned rejectSky;       /* traced: sky not flat within the bound */
     unsigned skySampled;      /* anchored form: pixels whose sky flatness needed the sampled test */
+    unsigned anchorsIncomplete; /* anchored form: anchors that spent the anchor step budget (traced
+                                   again in full, counted in rk4Pixels twice and in rejectAnchors) */
 } BHSurrogateStats;
 cudaError_t bhSurrogateFrameStats(BHSurrogate* s, BHSurrogateStats* stats);
 

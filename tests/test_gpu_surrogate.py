@@ -206,7 +206,7 @@ def _render(net, P):
     assert net.L.bhSurrogateRender(net.h, _ptr(f.out), _ptr(f.accum), _ptr(f.bloomA), _ptr(f.bloomB), C.byref(P),
                                    _stream()) == 0
     torch.cuda.synchronize()
-    st = np.zeros(12, dtype=np.uint32)
+    st = np.zeros(16, dtype=np.uint32)
     assert net.L.bhSurrogateFrameStats(net.h, st.ctypes.data_as(C.c_void_p)) == 0
     return f.out.cpu().numpy(), f.accum.cpu().numpy(), st
 
@@ -241,25 +241,31 @@ def test_render_with_every_pixel_on_rk4_equals_plain_frame(cuda, derive, stride)
         P = _kn_scene(derive, 320, 180)
         out, acc, st = _render(net, P)
         pout, pacc = _plain(P)
-        assert st[0] == 320 * 180 and st[1] == 320 * 180
+        # anchors that spent the anchor pass's step budget are traced twice
+        assert st[0] == 320 * 180 and st[1] == 320 * 180 + st[12]
         assert np.array_equal(acc, pacc)
         assert np.array_equal(out, pout)
     finally:
         net.close()
 
 
-@pytest.mark.parametrize("w,h,stride,min_interp,scene", [(960, 540, 4, 0.5, "kn"), (960, 540, 8, 0.5, "kn"),
-                                                         (1003, 565, 8, 0.4, "kn"),   # ragged: tiles padded
-                                                         (1920, 1080, 8, 0.5, "kerr")])
-def test_anchored_frame_within_one_lsb_of_plain(cuda, derive, w, h, stride, min_interp, scene):
-    """Anchored form without the network gate: RK4 anchors every `stride` pixels,
-    the rest interpolated (or black inside the shadow) where the error bound and
-    the sky allow.  Most pixels are not traced, the frame is within +-1 LSB of the
-    plain frame on >= 99.9 % of pixels, anchors and traced pixels equal the plain
-    frame's bit for bit, and the tallies add up."""
+@pytest.mark.parametrize("w,h,stride,min_interp,scene,steps",
+                         [(960, 540, 4, 0.5, "kn", 600), (960, 540, 8, 0.5, "kn", 600),
+                          (960, 540, 8, 0.5, "kn", 0),       # anchors traced with the frame's maxSteps
+                          (960, 540, 8, 0.25, "kn", 250),    # a budget many anchors spend
+                          (1003, 565, 8, 0.4, "kn", 600),    # ragged: tiles padded
+                          (1920, 1080, 8, 0.5, "kerr", 600)])
+def test_anchored_frame_within_one_lsb_of_plain(cuda, derive, w, h, stride, min_interp, scene, steps):
+    """Anchored form without the network gate: RK4 anchors every `stride` pixels
+    (with a step budget of `steps`), the rest interpolated (or black inside the
+    shadow) where the error bound and the sky allow.  Most pixels are not
+    traced, the frame is within +-1 LSB of the plain frame on >= 99.9 % of
+    pixels, anchors (incomplete ones traced again) and traced pixels equal the
+    plain frame's bit for bit, and the tallies add up."""
     net = Net(5)
     try:
         _anchors(net, stride, use_net=0)
+        assert net.L.bhSurrogateSetAnchorSteps(net.h, steps) == 0
         # the 4K Kerr-Newman orbit scene, or frame 3 of the 1080p Kerr a* = 0.9 scene
         P = _kn_scene(derive, w, h, az=75.0) if scene == "kn" else scenes.kerr_pair_1080(derive, w, h)[3]
         out, acc, st = _render(net, P)
@@ -271,8 +277,13 @@ def test_anchored_frame_within_one_lsb_of_plain(cuda, derive, w, h, stride, min_
         assert anchors == ((w - 1) // stride + 1) * ((h - 1) // stride + 1)
         assert np.array_equal(acc[::stride, ::stride], pacc[::stride, ::stride])   # anchors: plain pixels
         assert st[7] > min_interp * n                                 # interpolated (or shadow)
-        assert st[7] + st[8] + st[9] + st[10] + anchors == n           # every pixel accounted for once
-        assert st[1] == n - st[7] + st[2]                              # traced: the rest + held-out
+        incomplete = int(st[12])
+        if steps == 250:
+            assert incomplete > anchors // 20
+        if steps == 0:                          # only rays that reach the frame's maxSteps
+            assert incomplete <= anchors // 1000
+        assert st[7] + st[8] + st[9] + st[10] + anchors - incomplete == n   # every pixel accounted for once
+        assert st[1] == n - st[7] + st[2] + incomplete                # traced: the rest + held-out
         assert 0 < st[11] <= st[7] + st[10]        # sampled sky test: interpolated or rejected by the sky
         assert float((d <= 1).mean()) >= 0.999
         assert st[3] <= max(2, st[2] // 100)                           # held-out sample over 1 LSB
@@ -333,7 +344,7 @@ def test_trained_surrogate_gain_over_plain_rk4(cuda, derive):
             assert n.L.bhSurrogateSetGate(n.h, *[C.c_float(g) for g in gate[:3]], gate[3]) == 0
             t = _timed(lambda: n.L.bhSurrogateRender(n.h, _ptr(fs.out), _ptr(fs.accum), _ptr(fs.bloomA),
                                                      _ptr(fs.bloomB), C.byref(P), _stream()))
-            st = np.zeros(12, dtype=np.uint32)
+            st = np.zeros(16, dtype=np.uint32)
             assert n.L.bhSurrogateFrameStats(n.h, st.ctypes.data_as(C.c_void_p)) == 0
             d = np.abs(fs.out.cpu().numpy().astype(int) - plain)[..., :3].max(-1)
             return t, 1.0 - st[1] / st[0], float((d <= 1).mean())
