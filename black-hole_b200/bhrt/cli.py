@@ -8,6 +8,8 @@
     python black-hole_b200/bhrt/cli.py render --scene kn1080 --repeat 5      (timing)
     python black-hole_b200/bhrt/cli.py batch --scene pair1080 --frames 16 --repeat 3   (one queue)
     python black-hole_b200/bhrt/cli.py mlp --rays 2097152 --repeat 3      (surrogate MLP timing)
+    python black-hole_b200/bhrt/cli.py surrogate --scene orbit4k --stride 8 --repeat 3 --out s.png
+                                                      (anchored surrogate frame vs the plain frame)
 
 Replaces the reference application's interactive loop (src/main.cpp): the
 orbit camera, body orientation and quality presets become arguments; frames
@@ -117,9 +119,54 @@ def time_mlp(rays, repeat):
     return times
 
 
+def render_surrogate(P, stride, use_net, repeat, out_path):
+    """The anchored (stride >= 2) or network (stride 0) surrogate frame of an untrained
+    network (the anchored form without its cell gate needs none), timed, against the
+    plain frame: returns (times, plain ms, fraction within 1 LSB, frame statistics)."""
+    import ctypes as C
+    import numpy as np
+    import torch
+    from bhrt.device import Frame
+    from bhrt.imageio import write_image
+    L = lib.load()
+    h = C.c_void_p()
+    lib.check(L.bhSurrogateCreate(C.byref(h), 7), "bhSurrogateCreate")
+    try:
+        lib.check(L.bhSurrogateSetAnchors(h, stride, use_net, C.c_float(1e-4), C.c_float(0.5)), "anchors")
+        plain, f = Frame(P.width, P.height), Frame(P.width, P.height)
+        sp = C.c_void_p(torch.cuda.current_stream().cuda_stream)
+        e0, e1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+        plain.pipeline(P)
+        e0.record()
+        plain.pipeline(P)
+        e1.record()
+        torch.cuda.synchronize()
+        plain_ms = e0.elapsed_time(e1)
+        times = []
+        for _ in range(max(1, repeat)):
+            e0.record()
+            lib.check(L.bhSurrogateRender(h, C.c_void_p(f.out.data_ptr()), C.c_void_p(f.accum.data_ptr()),
+                                          C.c_void_p(f.bloomA.data_ptr()), C.c_void_p(f.bloomB.data_ptr()),
+                                          C.byref(P), sp), "bhSurrogateRender")
+            e1.record()
+            torch.cuda.synchronize()
+            times.append(e0.elapsed_time(e1))
+        st = np.zeros(16, dtype=np.uint32)
+        lib.check(L.bhSurrogateFrameStats(h, st.ctypes.data_as(C.c_void_p)), "bhSurrogateFrameStats")
+        d = (plain.out[..., :3].int() - f.out[..., :3].int()).abs().amax(dim=-1)
+        within = float((d <= 1).float().mean())
+        if out_path:
+            write_image(out_path, f.out.cpu().numpy())
+        return times, plain_ms, within, st
+    finally:
+        L.bhSurrogateDestroy(h)
+
+
 def main(argv=None):
     ap = argparse.ArgumentParser(description=__doc__, formatter_class=argparse.RawDescriptionHelpFormatter)
-    ap.add_argument("cmd", choices=["render", "sweep", "batch", "mlp", "info"])
+    ap.add_argument("cmd", choices=["render", "sweep", "batch", "mlp", "surrogate", "info"])
+    ap.add_argument("--stride", type=int, default=8, help="surrogate: anchor stride (0: the network form)")
+    ap.add_argument("--net", type=int, default=0, help="surrogate: 1 applies the network's gate (untrained)")
     ap.add_argument("--rays", type=int, default=3840 * 2160)
     ap.add_argument("--scene", default=None, help="schw320 | kerr1080 | kn1080 | pair1080 | kn4k | orbit4k | batch")
     ap.add_argument("--frame", type=int, default=0)
@@ -167,6 +214,13 @@ def main(argv=None):
         flop = 2.0 * (4 * 256 * 256 + 256 * 16) * a.rays
         print(f"fused surrogate MLP, {a.rays} rays: {min(t):.3f} ms (best of {len(t)}), "
               f"{flop / min(t) / 1e9:.1f} TFLOP/s")
+        return 0
+    if a.cmd == "surrogate":
+        P = named(a.scene, a.frame, a.width, a.height) if a.scene else custom(a)
+        t, pm, within, st = render_surrogate(P, a.stride, a.net, a.repeat, a.out)
+        print(f"{P.width}x{P.height} surrogate stride {a.stride}: {min(t):.3f} ms (best of {len(t)}), "
+              f"plain {pm:.3f} ms, {100 * within:.3f} % within 1 LSB, {st[7]} interpolated, "
+              f"{st[1]} traced by RK4" + (f" -> {a.out}" if a.out else ""))
         return 0
     if a.cmd == "batch":
         views = [named(a.scene, k, a.width, a.height) if a.scene else custom(a)

@@ -184,7 +184,7 @@ constexpr int kAncCols = 19, kAncRows = 8;
 // (4 tiles across, 2 down).
 // The block's anchors (escape direction and flags) are staged in shared memory
 // once; each pixel then reads its 4 x 4 neighbourhood from there.
-__global__ void __launch_bounds__(256) anchor_resolve_kernel(const __grid_constant__ SgAnchorFrame F)
+__global__ void __launch_bounds__(256, 4) anchor_resolve_kernel(const __grid_constant__ SgAnchorFrame F)
 {
     __shared__ float4 sAnc[kAncRows][kAncCols];
     const TraceParams& P = F.tp;
@@ -238,16 +238,19 @@ __global__ void __launch_bounds__(256) anchor_resolve_kernel(const __grid_consta
                 sky = g.x >= F.minProb;
                 dark = g.y >= F.minProb;
             }
-            f3 d[4][4];
+            // anchor (cx - 1 + i, cy - 1 + j) is staged at sAnc[cy - 1 + j - ay0][cx - 1 + i - ax0];
+            // the flags first, the directions re-read from shared memory where needed (keeps
+            // the 16 directions out of registers)
+            const float4(*st)[kAncCols] = reinterpret_cast<const float4(*)[kAncCols]>(&sAnc[cy - 1 - ay0][0]);
+            const int c0i = cx - 1 - ax0;
 #pragma unroll
             for (int j = 0; j < 4; ++j)
 #pragma unroll
                 for (int i = 0; i < 4; ++i)
-                {   // anchor (cx - 1 + i, cy - 1 + j), staged at (cy - 1 + j - ay0, cx - 1 + i - ax0)
-                    const float4 a = sAnc[cy - 1 + j - ay0][cx - 1 + i - ax0];
-                    sky = sky && __float_as_uint(a.w) == BH_ANCHOR_ESCAPED;
-                    dark = dark && __float_as_uint(a.w) == BH_ANCHOR_HORIZON;
-                    d[j][i] = v3(a.x, a.y, a.z);
+                {
+                    const unsigned fl = __float_as_uint(st[j][c0i + i].w);
+                    sky = sky && fl == BH_ANCHOR_ESCAPED;
+                    dark = dark && fl == BH_ANCHOR_HORIZON;
                 }
             reason = 1;
             if (dark)
@@ -270,12 +273,14 @@ __global__ void __launch_bounds__(256) anchor_resolve_kernel(const __grid_consta
                     for (int i = 0; i < 4; ++i)
                     {
                         const float w = wy[j] * wx[i];
-                        bc = v3(bc.x + w * d[j][i].x, bc.y + w * d[j][i].y, bc.z + w * d[j][i].z);
+                        const float4 a = st[j][c0i + i];
+                        bc = v3(bc.x + w * a.x, bc.y + w * a.y, bc.z + w * a.z);
                     }
-                const f3 top = v3(d[1][1].x + tx * (d[1][2].x - d[1][1].x), d[1][1].y + tx * (d[1][2].y - d[1][1].y),
-                                  d[1][1].z + tx * (d[1][2].z - d[1][1].z));
-                const f3 bot = v3(d[2][1].x + tx * (d[2][2].x - d[2][1].x), d[2][1].y + tx * (d[2][2].y - d[2][1].y),
-                                  d[2][1].z + tx * (d[2][2].z - d[2][1].z));
+                const float4 a11 = st[1][c0i + 1], a12 = st[1][c0i + 2], a21 = st[2][c0i + 1], a22 = st[2][c0i + 2];
+                const f3 top = v3(a11.x + tx * (a12.x - a11.x), a11.y + tx * (a12.y - a11.y),
+                                  a11.z + tx * (a12.z - a11.z));
+                const f3 bot = v3(a21.x + tx * (a22.x - a21.x), a21.y + tx * (a22.y - a21.y),
+                                  a21.z + tx * (a22.z - a21.z));
                 const f3 bl = unit3(v3(top.x + ty * (bot.x - top.x), top.y + ty * (bot.y - top.y),
                                        top.z + ty * (bot.z - top.z)));
                 bc = unit3(bc);
