@@ -102,6 +102,7 @@ struct BHSurrogate
 {
     SgState S;
     cudaStream_t stream = nullptr;
+    cudaEvent_t evFork = nullptr, evJoin = nullptr;   // anchored frames: the cell gate beside the anchor pass
     // frame scratch
     unsigned* list = nullptr;
     size_t listCap = 0;
@@ -155,6 +156,8 @@ void freeAll(BHSurrogate* s)
                   s->cellPix, s->cellGate, s->sampleDir, s->samplePix, s->blockOrder};
     for (void* p : ps)
         if (p) cudaFree(p);
+    if (s->evFork) cudaEventDestroy(s->evFork);
+    if (s->evJoin) cudaEventDestroy(s->evJoin);
     if (s->stream) cudaStreamDestroy(s->stream);
     delete s;
 }
@@ -342,7 +345,17 @@ cudaError_t anchoredFrame(BHSurrogate* s, const RenderParams& P, float4* accum, 
     if (e != cudaSuccess) return e;
     const unsigned nA = (unsigned)(s->aNx * s->aNy);
     const unsigned nC = (unsigned)((s->aNx - 1) * (s->aNy - 1));
-    if (s->anchorNet && s->aNx > 1 && s->aNy > 1)
+    const bool gate = s->anchorNet && s->aNx > 1 && s->aNy > 1;
+    // the cell gate (network at the cell centres) needs nothing of the anchor pass: it runs on
+    // the surrogate's own stream beside it and takes the SMs the anchor pass's tail frees
+    if (gate && (e = cudaEventRecord(s->evFork, stream)) != cudaSuccess) return e;
+    TraceParams t = bh_frame_params(P, BH_OUT_ANCHOR, s->anchorRec);
+    if (s->anchorSteps > 0 && s->anchorSteps < t.maxSteps) t.maxSteps = s->anchorSteps;
+    t.pixList = s->anchorPix;
+    t.nRays = nA;
+    if ((e = bh_device_counter(&t.counter)) != cudaSuccess) return e;
+    if ((e = bh_launch_trace(t, BH_PREC_FP32, false, bh_family_blocks(P), stream)) != cudaSuccess) return e;
+    if (gate)
     {
         SgState& S_ = s->S;
         SgFrame F{};
@@ -351,14 +364,11 @@ cudaError_t anchoredFrame(BHSurrogate* s, const RenderParams& P, float4* accum, 
         F.evalPix = s->cellPix;
         F.gateOut = s->cellGate;
         SgInferArgs a{S_.W, S_.W + 4 * kHidW, S_.biasPacked, nullptr, nullptr, nC, S_.err};
-        if ((e = sg_infer_launch(a, &F, stream)) != cudaSuccess) return e;
+        if ((e = cudaStreamWaitEvent(s->stream, s->evFork, 0)) != cudaSuccess) return e;
+        if ((e = sg_infer_launch(a, &F, s->stream)) != cudaSuccess) return e;
+        if ((e = cudaEventRecord(s->evJoin, s->stream)) != cudaSuccess) return e;
+        if ((e = cudaStreamWaitEvent(stream, s->evJoin, 0)) != cudaSuccess) return e;
     }
-    TraceParams t = bh_frame_params(P, BH_OUT_ANCHOR, s->anchorRec);
-    if (s->anchorSteps > 0 && s->anchorSteps < t.maxSteps) t.maxSteps = s->anchorSteps;
-    t.pixList = s->anchorPix;
-    t.nRays = nA;
-    if ((e = bh_device_counter(&t.counter)) != cudaSuccess) return e;
-    if ((e = bh_launch_trace(t, BH_PREC_FP32, false, bh_family_blocks(P), stream)) != cudaSuccess) return e;
     SgAnchorFrame A{};
     A.tp = bh_frame_params(P, BH_OUT_ACCUM, accum);
     A.anchors = s->anchorRec;
@@ -423,6 +433,8 @@ cudaError_t bhSurrogateCreate(BHSurrogate** out, unsigned seed)
     const size_t pc = (size_t)SgLayout::count() * sizeof(float);
     cudaError_t e = cudaGetDevice(&S.device);
     if (e == cudaSuccess) e = cudaStreamCreateWithFlags(&s->stream, cudaStreamNonBlocking);
+    if (e == cudaSuccess) e = cudaEventCreateWithFlags(&s->evFork, cudaEventDisableTiming);
+    if (e == cudaSuccess) e = cudaEventCreateWithFlags(&s->evJoin, cudaEventDisableTiming);
     if (e == cudaSuccess) e = bh_device_alloc(reinterpret_cast<void**>(&S.params), pc);
     if (e == cudaSuccess) e = bh_device_alloc(reinterpret_cast<void**>(&S.grads), pc);
     if (e == cudaSuccess) e = bh_device_alloc(reinterpret_cast<void**>(&S.adamM), pc);
