@@ -254,7 +254,9 @@ def test_render_with_every_pixel_on_rk4_equals_plain_frame(cuda, derive, stride)
                           (960, 540, 8, 0.5, "kn", 0),       # anchors traced with the frame's maxSteps
                           (960, 540, 8, 0.25, "kn", 250),    # a budget many anchors spend
                           (1003, 565, 8, 0.4, "kn", 600),    # ragged: tiles padded
-                          (1920, 1080, 8, 0.5, "kerr", 600)])
+                          (1920, 1080, 8, 0.5, "kerr", 600),
+                          (960, 540, 8, 0.3, "schw", 600),   # the spherical family's tracer
+                          (960, 540, 8, 0.3, "rn", 600)])
 def test_anchored_frame_within_one_lsb_of_plain(cuda, derive, w, h, stride, min_interp, scene, steps):
     """Anchored form without the network gate: RK4 anchors every `stride` pixels
     (with a step budget of `steps`), the rest interpolated (or black inside the
@@ -266,8 +268,15 @@ def test_anchored_frame_within_one_lsb_of_plain(cuda, derive, w, h, stride, min_
     try:
         _anchors(net, stride, use_net=0)
         assert net.L.bhSurrogateSetAnchorSteps(net.h, steps) == 0
-        # the 4K Kerr-Newman orbit scene, or frame 3 of the 1080p Kerr a* = 0.9 scene
-        P = _kn_scene(derive, w, h, az=75.0) if scene == "kn" else scenes.kerr_pair_1080(derive, w, h)[3]
+        # the 4K Kerr-Newman orbit scene, frame 3 of the 1080p Kerr a* = 0.9 scene, or the same
+        # orbit camera on a Schwarzschild / Reissner-Nordstrom (q = 0.6) hole
+        if scene == "kn":
+            P = _kn_scene(derive, w, h, az=75.0)
+        elif scene == "kerr":
+            P = scenes.kerr_pair_1080(derive, w, h)[3]
+        else:
+            P = scenes.scene(derive, 0 if scene == "schw" else 1, 0.0, 0.0 if scene == "schw" else 0.6, w, h,
+                             25.0, 15.0, 45.0, az_deg=75.0)
         out, acc, st = _render(net, P)
         pout, pacc = _plain(P)
         n = w * h
