@@ -33,8 +33,10 @@ Mrays/s (one primary ray per pixel) over the whole job, and 4K frame ms.
              events, L2 flushed: frame ms and this build's speed-up over it.
   surrogate  (1 GPU; --no-surrogate skips it) the learned lensing surrogate
              on the same scene: training from RK4-traced rays, then
-             bhSurrogateRender vs the plain frame under the strict acceptance
-             gate (and a permissive one), pixels within +-1 LSB.
+             bhSurrogateRender vs the plain frame in its anchored and network
+             forms under the strict acceptance gate (and a permissive one),
+             pixels within +-1 LSB; and the default anchored form with two
+             frames in flight (two handles, two streams).
   mixed_precision_4k, batch_256_views, post_process, accuracy, kerr_pair_1080
              (1 GPU; --no-configs skips them) the other workloads: the
              near-extremal 4K elevation sweep (FP32 vs mixed precision, frame
@@ -410,6 +412,62 @@ SG_W, SG_H = 3840, 2160
 SG_FRAMES = (0, 50, 100, 150, 200, 250)        # of the 300-frame orbit (azimuth 360 k / 300 deg)
 
 
+def two_stream_frames(L, h, scene, fa):
+    """The default anchored form with two frames in flight: a second surrogate handle with the same
+    weights renders every other orbit frame on its own stream (the frames of a pair overlap, so one
+    frame's anchor pass and resolve passes fill the other's tails).  frame_ms = a pair's time / 2."""
+    import ctypes as C
+    import torch
+    from bhrt import lib
+    from bhrt.device import Frame
+    ptr = lambda t: C.c_void_p(t.data_ptr())  # noqa: E731
+    h2 = C.c_void_p()
+    lib.check(L.bhSurrogateCreate(C.byref(h2), 7), "bhSurrogateCreate")
+    try:
+        w = np.zeros(L.bhSurrogateParamCount(), dtype=np.float32)
+        lib.check(L.bhSurrogateGetParams(h, w.ctypes.data_as(C.c_void_p)), "bhSurrogateGetParams")
+        lib.check(L.bhSurrogateSetParams(h2, w.ctypes.data_as(C.c_void_p)), "bhSurrogateSetParams")
+        hs = (h, h2)
+        for hh in hs:
+            lib.check(L.bhSurrogateSetAnchors(hh, 8, 1, C.c_float(1e-4), C.c_float(0.5)), "anchors")
+            lib.check(L.bhSurrogateSetGate(hh, C.c_float(0.95), C.c_float(0.95), C.c_float(0.02), 256), "gate")
+        fs = (Frame(SG_W, SG_H), Frame(SG_W, SG_H))
+        ss = (torch.cuda.Stream(), torch.cuda.Stream())
+        cur = torch.cuda.current_stream()
+        e0, e1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+
+        def pair(Ps):
+            for s in ss:
+                s.wait_stream(cur)
+            for i in range(2):
+                lib.check(L.bhSurrogateRender(hs[i], ptr(fs[i].out), ptr(fs[i].accum), ptr(fs[i].bloomA),
+                                              ptr(fs[i].bloomB), C.byref(Ps[i]), C.c_void_p(ss[i].cuda_stream)),
+                          "bhSurrogateRender")
+            for s in ss:
+                cur.wait_stream(s)
+
+        ms, within = [], []
+        for k in range(0, len(SG_FRAMES), 2):
+            Ps = (scene(SG_FRAMES[k]), scene(SG_FRAMES[k + 1]))
+            pair(Ps)                                     # warm-up
+            torch.cuda.synchronize()
+            e0.record()
+            pair(Ps)
+            e1.record()
+            torch.cuda.synchronize()
+            ms.append(e0.elapsed_time(e1) / 2)
+            for i in range(2):
+                fa.pipeline(Ps[i])
+                d = (fa.out[..., :3].int() - fs[i].out[..., :3].int()).abs().amax(dim=-1)
+                within.append(float((d <= 1).float().mean()))
+            torch.cuda.synchronize()
+        return {"gate": {"anchor_stride": 8, "network_cell_gate": True, "min_prob": 0.95, "min_conf": 0.95,
+                         "crit_band": 0.02, "held_stride": 256, "frames_in_flight": 2},
+                "frame_ms": float(np.median(ms)), "px_within_1lsb": float(np.min(within))}
+    finally:
+        L.bhSurrogateDestroy(h2)
+
+
 def surrogate_leg():
     import ctypes as C
     import torch
@@ -505,6 +563,7 @@ def surrogate_leg():
                           "px_within_1lsb": float(np.min(within)),
                           "rk4_pixel_frac": float(np.mean(rk4)),
                           "held_out": held, "held_out_over_1lsb": held_bad}
+        res["anchored_strict_two_streams"] = two_stream_frames(L, h, scene, fa)
         pm = float(np.median(plain_ms))
         for r in res.values():
             r["speedup_vs_plain"] = pm / r["frame_ms"]
@@ -740,7 +799,7 @@ def highlights(out):
     if sg:
         for g, r in sg["gates"].items():
             h[f"surrogate_{g}"] = {"frame_ms": r["frame_ms"], "speedup": r["speedup_vs_plain"],
-                                   "px_within_1lsb": r["px_within_1lsb"], "rk4_frac": r["rk4_pixel_frac"]}
+                                   "px_within_1lsb": r["px_within_1lsb"], "rk4_frac": r.get("rk4_pixel_frac")}
         h["surrogate_mlp_frac"] = sg["mlp"]["roofline"]["frac"]
     mx = out.get("mixed_precision_4k")
     if mx:
