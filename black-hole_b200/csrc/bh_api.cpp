@@ -127,7 +127,12 @@ cudaError_t tileOrder(int W, int H, const unsigned** out)
             c.dev = static_cast<unsigned*>(p);
             c.cap = n;
         }
+        // the table is shared by every stream: no frame may still read the old one, and the
+        // upload (a pageable copy, whose transfer can outlast the call) must be complete before
+        // a kernel on any stream reads it
+        if ((e = cudaDeviceSynchronize()) != cudaSuccess) return e;
         e = cudaMemcpy(c.dev, order.data(), n * sizeof(unsigned), cudaMemcpyHostToDevice);
+        if (e == cudaSuccess) e = cudaDeviceSynchronize();
         if (e != cudaSuccess) return e;
         c.W = W;
         c.H = H;

@@ -463,8 +463,10 @@ template <class V> BH_DEV void vfma_pair(V a, V x0, V x1, V y0, V y1, V& o0, V& 
 
 // V = float or double (one ray), float2 (two FP32 rays packed); S = the frame's
 // scalar type.  Every operation explicit, so one ray and a packed pair give the
-// same bits.
-template <class V, class S>
+// same bits.  SCALED = false: the five derivatives without their common factor
+// 1 / Sigma (returned in iS), for RK4 stages that fold it into the stage's
+// coefficients.
+template <class V, class S, bool SCALED = true>
 BH_DEV KerrEval<V> kerr_rhs(const CamFrame<S>& F, const KerrConsts<V>& k, V r, V s, V c, V pr, V pth)
 {
     const V M = lane<V>(F.M), a2 = lane<V>(F.a2);
@@ -486,13 +488,27 @@ BH_DEV KerrEval<V> kerr_rhs(const CamFrame<S>& F, const KerrConsts<V>& k, V r, V
     const V rmM = vsub(r, M);                                              // dDelta/dr / 2
     const V Wrh = vmul(PiD, vfma(PiD, rmM, vneg(vmul(k.twoE, r))));        // dW/dr / 2 = -P/D (dP - P/D dDelta) / 2
     const V KiS = vmul(o.K, iS);
-    o.d.r = vmul(Dpr, iS);
-    o.d.th = vmul(pth, iS);
-    o.d.ph = vmul(vfma(lane<V>(F.a), PiD, vfma(k.Lz, is2, vneg(k.aE))), iS);
+    const V uph = vfma(lane<V>(F.a), PiD, vfma(k.Lz, is2, vneg(k.aE)));
     // dpr = -(dH/dr) = (r K / Sigma - (dDelta pr^2 + dW/dr) / 2) / Sigma
-    o.d.pr = vmul(iS, vfma(vneg(vmul(rmM, pr)), pr, vfma(r, KiS, vneg(Wrh))));
+    const V upr = vfma(vneg(vmul(rmM, pr)), pr, vfma(r, KiS, vneg(Wrh)));
     // dpth = -(dH/dth) = cos (B (Lz / s^2 + a E) - a^2 s K / Sigma) / Sigma
-    o.d.pth = vmul(vmul(c, iS), vfma(B, vfma(k.Lz, is2, k.aE), vneg(vmul(vmul(a2, s), KiS))));
+    const V upth = vfma(B, vfma(k.Lz, is2, k.aE), vneg(vmul(vmul(a2, s), KiS)));
+    if constexpr (SCALED)
+    {
+        o.d.r = vmul(Dpr, iS);
+        o.d.th = vmul(pth, iS);
+        o.d.ph = vmul(uph, iS);
+        o.d.pr = vmul(iS, upr);
+        o.d.pth = vmul(vmul(c, iS), upth);
+    }
+    else
+    {
+        o.d.r = Dpr;
+        o.d.th = pth;
+        o.d.ph = uph;
+        o.d.pr = upr;
+        o.d.pth = vmul(c, upth);
+    }
     o.Pp = Pp;
     o.iDelT = vsel_ge(DelRaw, lane<V>((S)1e-5f), iDel, lane<V>((S)1e5f));
     o.iS = iS;
@@ -501,37 +517,47 @@ BH_DEV KerrEval<V> kerr_rhs(const CamFrame<S>& F, const KerrConsts<V>& k, V r, V
 
 // The classic RK4 step of the Kerr-Newman system from the state (r, th, ph,
 // pr, pth) with step h and first right-hand side d1; d4 receives the final
-// stage's derivative.  (reference src/trace.cuh:811-838)
+// stage's derivative without its factor 1 / Sigma, iS4 that factor.
+// (reference src/trace.cuh:811-838)  Stages 2-4 evaluate the right-hand side
+// unscaled and fold 1 / Sigma into the stage's coefficients (2 / Sigma for the
+// weighted sum, h / (2 Sigma) or h / Sigma for the next stage point), which
+// saves the five products by 1 / Sigma per stage.
 template <class V, class S>
 BH_DEV void kerr_rk4(const CamFrame<S>& F, const KerrConsts<V>& k, V h, V& r, V& th, V& ph, V& pr, V& pth,
-                     const KerrDeriv<V>& d1, KerrDeriv<V>& d4)
+                     const KerrDeriv<V>& d1, KerrDeriv<V>& d4, V& iS4)
 {
     const V hh = vmul(lane<V>((S)0.5f), h), two = lane<V>((S)2.f);
     V sx, cx, yr, yth, ypr, ypth;
     vfma_pair(hh, d1.r, d1.th, r, th, yr, yth);
     vfma_pair(hh, d1.pr, d1.pth, pr, pth, ypr, ypth);
     vsincos_stage(yth, sx, cx);
-    const KerrDeriv<V> d2 = kerr_rhs(F, k, yr, sx, cx, ypr, ypth).d;
-    V sr, sth, spr, spth, sph = vfma(two, d2.ph, d1.ph);
-    vfma_pair(two, d2.r, d2.th, d1.r, d1.th, sr, sth);
-    vfma_pair(two, d2.pr, d2.pth, d1.pr, d1.pth, spr, spth);
-    vfma_pair(hh, d2.r, d2.th, r, th, yr, yth);
-    vfma_pair(hh, d2.pr, d2.pth, pr, pth, ypr, ypth);
+    KerrEval<V> e = kerr_rhs<V, S, false>(F, k, yr, sx, cx, ypr, ypth);      // stage 2
+    V w = vmul(two, e.iS), a = vmul(hh, e.iS);
+    V sr, sth, spr, spth, sph = vfma(w, e.d.ph, d1.ph);
+    vfma_pair(w, e.d.r, e.d.th, d1.r, d1.th, sr, sth);
+    vfma_pair(w, e.d.pr, e.d.pth, d1.pr, d1.pth, spr, spth);
+    vfma_pair(a, e.d.r, e.d.th, r, th, yr, yth);
+    vfma_pair(a, e.d.pr, e.d.pth, pr, pth, ypr, ypth);
     vsincos_stage(yth, sx, cx);
-    const KerrDeriv<V> d3 = kerr_rhs(F, k, yr, sx, cx, ypr, ypth).d;
-    vfma_pair(two, d3.r, d3.th, sr, sth, sr, sth);
-    vfma_pair(two, d3.pr, d3.pth, spr, spth, spr, spth);
-    sph = vfma(two, d3.ph, sph);
-    vfma_pair(h, d3.r, d3.th, r, th, yr, yth);
-    vfma_pair(h, d3.pr, d3.pth, pr, pth, ypr, ypth);
+    e = kerr_rhs<V, S, false>(F, k, yr, sx, cx, ypr, ypth);                  // stage 3
+    w = vmul(two, e.iS);
+    a = vmul(h, e.iS);
+    vfma_pair(w, e.d.r, e.d.th, sr, sth, sr, sth);
+    vfma_pair(w, e.d.pr, e.d.pth, spr, spth, spr, spth);
+    sph = vfma(w, e.d.ph, sph);
+    vfma_pair(a, e.d.r, e.d.th, r, th, yr, yth);
+    vfma_pair(a, e.d.pr, e.d.pth, pr, pth, ypr, ypth);
     vsincos_stage(yth, sx, cx);
-    d4 = kerr_rhs(F, k, yr, sx, cx, ypr, ypth).d;
+    e = kerr_rhs<V, S, false>(F, k, yr, sx, cx, ypr, ypth);                  // stage 4
+    d4 = e.d;
+    iS4 = e.iS;
     const V h6 = vmul(h, lane<V>((S)(1.0 / 6.0)));
     V t0, t1, t2, t3;
-    t0 = vadd(sr, d4.r); t1 = vadd(sth, d4.th); t2 = vadd(spr, d4.pr); t3 = vadd(spth, d4.pth);
+    vfma_pair(iS4, d4.r, d4.th, sr, sth, t0, t1);
+    vfma_pair(iS4, d4.pr, d4.pth, spr, spth, t2, t3);
     vfma_pair(h6, t0, t1, r, th, r, th);
     vfma_pair(h6, t2, t3, pr, pth, pr, pth);
-    ph = vfma(h6, vadd(sph, d4.ph), ph);
+    ph = vfma(h6, vfma(iS4, d4.ph, sph), ph);
 }
 
 // One RK4 step of the Kerr-Newman system in FP64 from an FP32 state (the
@@ -718,13 +744,14 @@ struct KerrRay
                 KerrStep64 o = kerr_rk4_fp64(P.cd, k.E, k.Lz, r, th, ph, pr, pth, h);
                 r = o.r; th = o.th; ph = o.ph; pr = o.pr; pth = o.pth;
                 dl0 = o.dr4; dl1 = o.dth4; dl2 = o.dph4;
-                return finish_step(P, F, h, rS, thS, drS, dthS, dl0, dl1, dl2);
+                return finish_step(P, F, h, rS, thS, drS, dthS, dl0, dl1, dl2, R(1));
             }
         }
 
         KerrDeriv<R> d4;
-        kerr_rk4(F, k, h, r, th, ph, pr, pth, d1, d4);
-        return finish_step(P, F, h, rS, thS, drS, dthS, d4.r, d4.th, d4.ph);
+        R iS4;
+        kerr_rk4(F, k, h, r, th, ph, pr, pth, d1, d4, iS4);
+        return finish_step(P, F, h, rS, thS, drS, dthS, d4.r, d4.th, d4.ph, iS4);
     }
 
     BH_DEV bool polar_passage_fp64(const TraceParams& P);
@@ -732,7 +759,7 @@ struct KerrRay
     // Rest of a loop iteration after the RK4 update: pole guard, the next
     // step's first right-hand side with the slow-light term, disk chord.
     BH_DEV bool finish_step(const TraceParams& P, const CamFrame<R>& F, R h, R rS, R thS, R drS, R dthS,
-                            R d4r, R d4th, R d4ph)
+                            R d4r, R d4th, R d4ph, R d4iS)
     {
         // pole reflection guard
         if (th < R(1e-3f)) { th = R(1e-3f); pth = abs_p(pth); }
@@ -740,8 +767,8 @@ struct KerrRay
         ++step;
         if (step == P.maxSteps)
         {
-            R* dl = last_deriv();
-            dl[0] = d4r; dl[1] = d4th; dl[2] = d4ph;
+            R* dl = last_deriv();      // the final stage's derivative, scaled by 1 / Sigma
+            dl[0] = d4r * d4iS; dl[1] = d4th * d4iS; dl[2] = d4ph * d4iS;
         }
 
         // next step's first right-hand side; its Sigma, Delta, P give the slow

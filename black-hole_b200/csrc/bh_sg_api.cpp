@@ -224,15 +224,16 @@ cudaError_t criticalCurve(BHSurrogate* s, const RenderParams& P0, float* crit)
 // Frame scratch of a W x H frame.  The RK4 list holds whole 32-entry groups
 // (8x4 tiles in the anchored form, 32 consecutive pixels in the network form),
 // bounded by the frame padded to whole tiles or whole groups; then, in the
-// anchored form, the deferred pixels the sampled sky test rejects (at most
-// sampleCap, a quarter of the frame: more are traced in their tiles); then the
-// held-out sample (at most heldCap pixels).
+// anchored form, the deferred pixels the sampled sky test rejects; then the
+// held-out sample (at most heldCap pixels).  The deferral buffer holds every
+// pixel of the frame (20 bytes each), so which pixels are deferred, and hence
+// the frame, never depends on the order of the resolve pass's atomics.
 cudaError_t ensureFrame(BHSurrogate* s, int W, int H)
 {
     const size_t pixels = (size_t)W * H;
     const size_t stride = s->heldStride > 0 ? (size_t)s->heldStride : pixels + 1;
     const size_t want = std::min(pixels, pixels / stride * 2 + 4096);
-    const size_t sampleCap = std::min(pixels, pixels / 4 + 4096);
+    const size_t sampleCap = pixels;
     const size_t listLen =
         std::max((size_t)((W + 7) / 8 * 8) * (size_t)((H + 3) / 4 * 4), (pixels + 31) / 32 * 32) + sampleCap + want;
     if (listLen <= s->listCap && want <= s->heldCap && sampleCap <= s->sampleCap) return cudaSuccess;
@@ -309,6 +310,9 @@ cudaError_t ensureAnchors(BHSurrogate* s, int W, int H, int S)
     for (int y = 0; y + 1 < ny; ++y)
         for (int x = 0; x + 1 < nx; ++x)
             c[(size_t)y * (nx - 1) + x] = (unsigned)(y * S + S / 2) * (unsigned)W + (unsigned)(x * S + S / 2);
+    // blocking upload: no earlier frame of this handle may still read the tables, and the
+    // pageable copies must have landed before a kernel on any stream reads them
+    if ((e = cudaDeviceSynchronize())) return e;
     if ((e = cudaMemcpy(s->anchorPix, a.data(), nA * sizeof(unsigned), cudaMemcpyHostToDevice))) return e;
     if ((e = cudaMemcpy(s->anchorSlot, slot.data(), nA * sizeof(unsigned), cudaMemcpyHostToDevice))) return e;
     // resolve blocks (32 x 8 pixels) nearest the screen centre first
@@ -332,6 +336,7 @@ cudaError_t ensureAnchors(BHSurrogate* s, int W, int H, int S)
     }
     if ((e = cudaMemcpy(s->blockOrder, blocks.data(), nB * sizeof(unsigned), cudaMemcpyHostToDevice))) return e;
     if ((e = cudaMemcpy(s->cellPix, c.data(), nC * sizeof(unsigned), cudaMemcpyHostToDevice))) return e;
+    if ((e = cudaDeviceSynchronize())) return e;
     s->aW = W; s->aH = H; s->aS = S; s->aNx = nx; s->aNy = ny;
     return cudaSuccess;
 }

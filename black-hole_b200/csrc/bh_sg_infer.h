@@ -80,7 +80,8 @@ struct SgAnchorFrame
     unsigned frameSeed;
     float4* sampleDir;              // deferred pixels: (interpolated direction, error bound)
     unsigned* samplePix;
-    unsigned* sampleCount;          // deferred pixels claimed (beyond sampleCap: traced instead)
+    unsigned* sampleCount;          // deferred pixels claimed (beyond sampleCap, which the host sizes
+                                    // to the whole frame: traced instead)
     unsigned sampleCap;
     unsigned* stats;                // [0] interpolated, [1] rejected by the anchors / cell gate,
                                     // [2] by the error bound, [3] by the sky sensitivity,

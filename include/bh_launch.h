@@ -174,8 +174,10 @@ void bhGetTuning(int family, int* refillMin, int* blocksPerSm);
 /* Order in which the 8x4-pixel tiles of a frame are traced: 0 row-major,
  * 1 centre-out (default; the shadow and photon ring first, so the frame ends on
  * short escaping rays).  The table is built once per device and resolution on
- * the first call at that resolution (a blocking upload: make that first call
- * outside any stream capture).  Returns 1 when applied, 0 when out of range. */
+ * the first call at that resolution (a blocking upload that first waits for
+ * all work on the device, since frames of the previous resolution may still
+ * read the table: make that first call outside any stream capture).  Returns
+ * 1 when applied, 0 when out of range. */
 int bhSetTileOrder(int mode);
 int bhGetTileOrder(void);
 

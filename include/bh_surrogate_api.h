@@ -136,7 +136,11 @@ cudaError_t bhSurrogateTrain(BHSurrogate* s, int steps, int batch, float lr, uns
  *    distance, inclination and field of view and cached -- that first call
  *    blocks); the rest go through the RK4 tracer.
  * In both forms a held-out sample of 1 in 256 of the resolved pixels is also
- * traced and compared, then bloom and tonemap run. */
+ * traced and compared, then bloom and tonemap run.  The first anchored frame
+ * of a handle at a size and stride builds its tables (a blocking upload that
+ * waits for all work on the device).  A handle's scratch is its own: two
+ * handles may render on two streams at once (two frames in flight); one
+ * handle must not render on two streams at once. */
 cudaError_t bhSurrogateRender(BHSurrogate* s, uchar4* out, float4* accum, float4* bloomA, float4* bloomB,
                               const RenderParams* p, cudaStream_t stream);
 

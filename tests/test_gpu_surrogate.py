@@ -375,3 +375,33 @@ def test_trained_surrogate_gain_over_plain_rk4(cuda, derive):
     finally:
         net.close()
         raw.close()
+
+
+def test_two_handles_on_two_streams_match_one_handle(cuda, derive):
+    """Two frames in flight: two surrogate handles rendering on two streams at once give the
+    frames one handle renders one after the other, bit for bit (each handle's scratch is its
+    own; the held-out sample, which differs with a handle's frame count, is off)."""
+    import torch
+    nets = [Net(5), Net(5)]
+    try:
+        for net in nets:
+            _anchors(net, 8, use_net=0)
+            assert net.L.bhSurrogateSetGate(net.h, C.c_float(0.95), C.c_float(0.95), C.c_float(0.02), 0) == 0
+        Ps = [_kn_scene(derive, 960, 540, az=a) for a in (30.0, 75.0)]
+        seq = [_render(nets[0], P)[1].copy() for P in Ps]
+        fs = [Frame(960, 540), Frame(960, 540)]
+        ss = [torch.cuda.Stream(), torch.cuda.Stream()]
+        for rep in range(2):
+            for i in range(2):
+                ss[i].wait_stream(torch.cuda.current_stream())
+                assert nets[i].L.bhSurrogateRender(nets[i].h, _ptr(fs[i].out), _ptr(fs[i].accum), _ptr(fs[i].bloomA),
+                                                   _ptr(fs[i].bloomB), C.byref(Ps[i]),
+                                                   C.c_void_p(ss[i].cuda_stream)) == 0
+            torch.cuda.synchronize()
+            for i in range(2):
+                a = fs[i].accum.cpu().numpy()
+                bad = np.argwhere((a != seq[i]).any(axis=-1))
+                assert len(bad) == 0, (rep, i, len(bad), bad[:8].tolist())
+    finally:
+        for net in nets:
+            net.close()
