@@ -205,6 +205,22 @@ cudaError_t bh_gemm_bf16(const void* A, int lda, const void* B, int ldb, float* 
 // ---------------------------------------------------------------------------
 namespace {
 __device__ unsigned gTcError;
+
+// Self-check of the bounded barrier waits: one thread waits for a phase of a
+// barrier that nothing arrives at; the wait gives up after limitNs, sets bit 0
+// of the error word and the kernel returns (no copy or tensor-memory state is
+// involved, so nothing is left in flight).
+__global__ void wait_probe_kernel(unsigned* err, unsigned long long limitNs)
+{
+    __shared__ uint64_t bar;
+    if (threadIdx.x == 0)
+    {
+        mbar_init(&bar, 1);
+        fence_barrier_init();
+    }
+    __syncthreads();
+    if (threadIdx.x == 0) mbar_wait(&bar, 0, err, limitNs);
+}
 }
 
 cudaError_t bh_tc_error_word(unsigned** out)
@@ -219,6 +235,16 @@ extern "C" cudaError_t bhTcGemm(const void* A, int lda, const void* B, int ldb, 
     cudaError_t e = bh_tc_error_word(&err);
     if (e != cudaSuccess) return e;
     return bh_gemm_bf16(A, lda, B, ldb, C, ldc, M, N, K, splits, accumulate != 0, bias, err, stream);
+}
+
+extern "C" cudaError_t bhTcWaitProbe(int limitUs, cudaStream_t stream)
+{
+    if (limitUs < 1 || limitUs > 1000000) return cudaErrorInvalidValue;
+    unsigned* err = nullptr;
+    cudaError_t e = bh_tc_error_word(&err);
+    if (e != cudaSuccess) return e;
+    wait_probe_kernel<<<1, 32, 0, stream>>>(err, (unsigned long long)limitUs * 1000ull);
+    return cudaGetLastError();
 }
 
 extern "C" cudaError_t bhTcErrorFlags(unsigned* flags)

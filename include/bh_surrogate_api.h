@@ -37,6 +37,12 @@ cudaError_t bhTcGemm(const void* A, int lda, const void* B, int ldb, float* C, i
  * a bounded wait inside a kernel timed out (its results are invalid). */
 cudaError_t bhTcErrorFlags(unsigned* flags);
 
+/* Self-check of that error path: one kernel waits (bounded, limitUs
+ * microseconds, 1 .. 1e6) on a barrier phase that nothing completes, so the
+ * wait gives up, sets bit 0 of the flags and the kernel returns; the next
+ * bhTcErrorFlags reports it.  The device stays usable. */
+cudaError_t bhTcWaitProbe(int limitUs, cudaStream_t stream);
+
 /* ---- the network -------------------------------------------------------------
  * Inputs, one row of 8 floats per ray: the unit ray direction in the camera
  * basis (right, up, forward components), a* in [-1, 1], (q - 0.3) / 0.3,

@@ -51,3 +51,20 @@ def test_tc_gemm_matches_float64(cuda, M, N, K, splits, acc, bias):
     print(f"M={M} N={N} K={K} splits={splits}: max abs err {err:.3g} (scale {scale:.3g})")
     # FP32 accumulation of K exact BF16 products: error ~ K * 2^-24 * |terms|
     assert err <= 1e-5 * K * 4.0 + 1e-4
+
+
+def test_bounded_wait_times_out_reports_and_device_stays_usable(cuda):
+    """A barrier wait that nothing completes gives up after its limit (1 ms here), sets the
+    error flag that bhTcErrorFlags reads (and clears), and leaves the device usable: a GEMM
+    right after it is exact and raises no flag."""
+    import torch
+    L = lib.load()
+    flags = C.c_uint(99)
+    assert L.bhTcErrorFlags(C.byref(flags)) == 0
+    assert L.bhTcWaitProbe(0, None) != 0 and L.bhTcWaitProbe(2000000, None) != 0   # limits out of range
+    assert L.bhTcWaitProbe(1000, C.c_void_p(torch.cuda.current_stream().cuda_stream)) == 0
+    torch.cuda.synchronize()
+    assert L.bhTcErrorFlags(C.byref(flags)) == 0 and flags.value & 1
+    assert L.bhTcErrorFlags(C.byref(flags)) == 0 and flags.value == 0
+    err, scale = _run(256, 256, 256)
+    assert err <= 1e-5 * 256 * 4.0 + 1e-4
