@@ -654,7 +654,10 @@ cudaError_t bhSurrogateRender(BHSurrogate* s, uchar4* out, float4* accum, float4
     RenderParams P = *p;
     bhSanitizeRenderParams(&P);
     if (!out || !accum || (P.bloomEnabled && (!bloomA || !bloomB))) return cudaErrorInvalidValue;
-    if (std::fabs(P.camRight.y) > 1e-4f || P.accumMode != 0) return cudaErrorInvalidValue;
+    // the network's inputs assume an orbit camera; the anchored form without its cell
+    // gate works in screen space and takes any camera
+    const bool network = s->anchorStride < 2 || s->anchorNet;
+    if ((network && std::fabs(P.camRight.y) > 1e-4f) || P.accumMode != 0) return cudaErrorInvalidValue;
     const size_t pixels = (size_t)P.width * P.height;
     cudaError_t e = ensureFrame(s, P.width, P.height);
     if (e != cudaSuccess) return e;

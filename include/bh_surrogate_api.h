@@ -121,8 +121,10 @@ cudaError_t bhSurrogateDatasetCopy(BHSurrogate* s, float* in, float* tgt, long l
 cudaError_t bhSurrogateTrain(BHSurrogate* s, int steps, int batch, float lr, unsigned seed, float* lossHistory);
 
 /* Render one frame with the surrogate: same buffers and result layout as
- * launchRenderPipeline.  Requires an orbit camera (looking at the hole, no
- * roll: camRight.y == 0) and accumMode 0.  Two forms (bhSurrogateSetAnchors):
+ * launchRenderPipeline.  Requires accumMode 0, and wherever the network is
+ * evaluated (the network form, the anchored form's cell gate) an orbit camera
+ * (looking at the hole, no roll: camRight.y == 0); the anchored form without
+ * the cell gate takes any camera.  Two forms (bhSurrogateSetAnchors):
  *  - anchored (the default, anchor stride 8): the FP32 RK4 tracer traces one
  *    pixel in stride x stride (the anchors); a pixel between anchors takes the
  *    bicubic interpolation of the 4 x 4 surrounding anchors' escape directions

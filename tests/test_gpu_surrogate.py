@@ -256,7 +256,8 @@ def test_render_with_every_pixel_on_rk4_equals_plain_frame(cuda, derive, stride)
                           (1003, 565, 8, 0.4, "kn", 600),    # ragged: tiles padded
                           (1920, 1080, 8, 0.5, "kerr", 600),
                           (960, 540, 8, 0.3, "schw", 600),   # the spherical family's tracer
-                          (960, 540, 8, 0.3, "rn", 600)])
+                          (960, 540, 8, 0.3, "rn", 600),
+                          (960, 540, 8, 0.3, "rolled", 600)])   # any camera without the cell gate
 def test_anchored_frame_within_one_lsb_of_plain(cuda, derive, w, h, stride, min_interp, scene, steps):
     """Anchored form without the network gate: RK4 anchors every `stride` pixels
     (with a step budget of `steps`), the rest interpolated (or black inside the
@@ -274,6 +275,9 @@ def test_anchored_frame_within_one_lsb_of_plain(cuda, derive, w, h, stride, min_
             P = _kn_scene(derive, w, h, az=75.0)
         elif scene == "kerr":
             P = scenes.kerr_pair_1080(derive, w, h)[3]
+        elif scene == "rolled":   # body orientation (10, 25, 35) deg: the camera is rolled and tilted
+            P = scenes.scene(derive, 3, 0.8, 0.3, w, h, 25.0, 15.0, 45.0, az_deg=75.0, ori_deg=(10.0, 25.0, 35.0))
+            assert abs(P.camRight.y) > 0.1
         else:
             P = scenes.scene(derive, 0 if scene == "schw" else 1, 0.0, 0.0 if scene == "schw" else 0.6, w, h,
                              25.0, 15.0, 45.0, az_deg=75.0)
@@ -405,3 +409,18 @@ def test_two_handles_on_two_streams_match_one_handle(cuda, derive):
     finally:
         for net in nets:
             net.close()
+
+
+def test_network_forms_need_an_orbit_camera(cuda, derive):
+    """The network's inputs assume an orbit camera: with a rolled camera the network form and the
+    anchored form with its cell gate refuse the frame; the anchored form without the gate renders it."""
+    net = Net(5)
+    try:
+        P = scenes.scene(derive, 3, 0.8, 0.3, 320, 180, 25.0, 15.0, 45.0, az_deg=75.0, ori_deg=(10.0, 25.0, 35.0))
+        f = Frame(320, 180)
+        args = (_ptr(f.out), _ptr(f.accum), _ptr(f.bloomA), _ptr(f.bloomB), C.byref(P), _stream())
+        for stride, use_net, ok in ((0, 1, False), (8, 1, False), (8, 0, True)):
+            _anchors(net, stride, use_net=use_net)
+            assert (net.L.bhSurrogateRender(net.h, *args) == 0) == ok
+    finally:
+        net.close()
