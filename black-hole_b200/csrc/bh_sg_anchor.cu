@@ -128,6 +128,21 @@ __device__ __forceinline__ void push_tile(unsigned* list, unsigned* count, unsig
     list[base + lane] = want ? pix : BH_PIX_SKIP;
 }
 
+// The pixel's sample into the accumulation buffer, blended as the tracer blends it
+// (accum_blend: mode 0 replaces, modes 1 and 2 average over the frame sequence).
+__device__ __forceinline__ void write_sample(const TraceParams& P, unsigned pix, f3 hdr)
+{
+    float4* acc = reinterpret_cast<float4*>(P.out);
+    if (P.accumMode != 0 && P.sampleIndex > 0)
+    {
+        const float4 pv = acc[pix];
+        f3 prev = v3(pv.x, pv.y, pv.z);
+        if (!isfinite(prev.x) || !isfinite(prev.y) || !isfinite(prev.z)) prev = hdr;
+        hdr = accum_blend(prev, hdr, P.accumMode, P.sampleIndex);
+    }
+    acc[pix] = make_float4(hdr.x, hdr.y, hdr.z, 1.f);
+}
+
 // Warp-wide claim of one slot per lane that wants one (all lanes call it): the
 // lanes' slots are consecutive, in lane order, from one atomicAdd on `count`.
 __device__ __forceinline__ unsigned warp_claim(unsigned* count, bool want)
@@ -198,7 +213,6 @@ __global__ void __launch_bounds__(256, 4) anchor_resolve_kernel(const __grid_con
     const bool inFrame = x < P.W && y < P.H;
     const int S = F.S;
     const unsigned pix = inFrame ? (unsigned)y * (unsigned)P.W + (unsigned)x : 0u;
-    float4* acc = reinterpret_cast<float4*>(P.out);
     const int ax0 = (bx * 32) / S - 1, ay0 = (by * 8) / S - 1;
     for (int i = threadIdx.x; i < kAncRows * kAncCols; i += blockDim.x)
     {
@@ -312,7 +326,7 @@ __global__ void __launch_bounds__(256, 4) anchor_resolve_kernel(const __grid_con
         }
         else reason = 1;
     }
-    if (anchor || resolved) acc[pix] = make_float4(hdr.x, hdr.y, hdr.z, 1.f);
+    if (anchor || resolved) write_sample(P, pix, hdr);
 
     // deferred pixels to the sample buffer; beyond its capacity they are traced
     const unsigned k = warp_claim(F.sampleCount, defer);
@@ -337,7 +351,6 @@ __global__ void __launch_bounds__(256) sky_sample_kernel(const __grid_constant__
 {
     const TraceParams& P = F.tp;
     const unsigned n = min(*F.sampleCount, F.sampleCap);
-    float4* acc = reinterpret_cast<float4*>(P.out);
     const unsigned lane = threadIdx.x & 31u;
     for (unsigned base = blockIdx.x * blockDim.x; base < n; base += gridDim.x * blockDim.x)
     {
@@ -373,7 +386,7 @@ __global__ void __launch_bounds__(256) sky_sample_kernel(const __grid_constant__
                 flat = lum_exposed(ck, P.exposure) < kLumBloomSafe && fabsf(yk.x - y0.x) < F.maxStep &&
                        fabsf(yk.y - y0.y) < F.maxStep && fabsf(yk.z - y0.z) < F.maxStep;
             }
-            if (flat) acc[pix] = make_float4(c0.x, c0.y, c0.z, 1.f);
+            if (flat) write_sample(P, pix, c0);
         }
         const bool trace = valid && !flat;
         const unsigned m = __ballot_sync(0xffffffffu, trace);

@@ -390,7 +390,9 @@ cudaError_t anchoredFrame(BHSurrogate* s, const RenderParams& P, float4* accum, 
     A.heldPred = s->heldPred;
     A.heldCount = s->counters + 1;
     A.heldCap = s->heldCap;
-    A.heldStride = s->heldStride;
+    // under progressive accumulation the buffer holds the blend, not this frame's sample, so the
+    // held-out comparison (RK4 sample against the interpolated one) is off
+    A.heldStride = P.accumMode != 0 ? 0 : s->heldStride;
     A.frameSeed = ++s->frames;
     A.sampleDir = s->sampleDir;
     A.samplePix = s->samplePix;
@@ -657,7 +659,8 @@ cudaError_t bhSurrogateRender(BHSurrogate* s, uchar4* out, float4* accum, float4
     // the network's inputs assume an orbit camera; the anchored form without its cell
     // gate works in screen space and takes any camera
     const bool network = s->anchorStride < 2 || s->anchorNet;
-    if ((network && std::fabs(P.camRight.y) > 1e-4f) || P.accumMode != 0) return cudaErrorInvalidValue;
+    if (network && std::fabs(P.camRight.y) > 1e-4f) return cudaErrorInvalidValue;
+    if (s->anchorStride < 2 && P.accumMode != 0) return cudaErrorInvalidValue;
     const size_t pixels = (size_t)P.width * P.height;
     cudaError_t e = ensureFrame(s, P.width, P.height);
     if (e != cudaSuccess) return e;

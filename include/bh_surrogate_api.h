@@ -121,10 +121,13 @@ cudaError_t bhSurrogateDatasetCopy(BHSurrogate* s, float* in, float* tgt, long l
 cudaError_t bhSurrogateTrain(BHSurrogate* s, int steps, int batch, float lr, unsigned seed, float* lossHistory);
 
 /* Render one frame with the surrogate: same buffers and result layout as
- * launchRenderPipeline.  Requires accumMode 0, and wherever the network is
- * evaluated (the network form, the anchored form's cell gate) an orbit camera
- * (looking at the hole, no roll: camRight.y == 0); the anchored form without
- * the cell gate takes any camera.  Two forms (bhSurrogateSetAnchors):
+ * launchRenderPipeline.  Wherever the network is evaluated (the network
+ * form, the anchored form's cell gate) it requires an orbit camera (looking at
+ * the hole, no roll: camRight.y == 0); the anchored form without the cell gate
+ * takes any camera.  The network form requires accumMode 0; the anchored form
+ * also accumulates (modes 1 and 2 blend each pixel's sample as the tracer
+ * does, with the same sub-pixel jitter; the held-out sample is then off).
+ * Two forms (bhSurrogateSetAnchors):
  *  - anchored (the default, anchor stride 8): the FP32 RK4 tracer traces one
  *    pixel in stride x stride (the anchors); a pixel between anchors takes the
  *    bicubic interpolation of the 4 x 4 surrounding anchors' escape directions
