@@ -14,7 +14,7 @@
 //     cell centre escapes without the disk, >= minProb) passes, the bound is below
 //     epsMax, and the sky is flat within the bound: either no star of the
 //     four star lattices lies within reach of the bound (an exact test on the
-//     lattice cell and the cell's star), or the display values (exposure,
+//     lattice cells the bound reaches and their stars), or the display values (exposure,
 //     ACES, vibrance, gamma, before dither, in byte units) of the sky at the
 //     direction and at four directions sqrt(2) bound away differ by less
 //     than maxStep; and the pixel stays below the bloom bright-pass
@@ -72,26 +72,48 @@ __device__ __forceinline__ float lum_exposed(f3 c, float exposure)
     return exposure * (0.2126f * c.x + 0.7152f * c.y + 0.0722f * c.z);
 }
 
+// Is the star of lattice cell `c` (integer coordinates; star_layer draws it only
+// inside that cell, where d2 * sharp <= cut) farther than m + its cut radius
+// from the point p (cell units)?  fc = p - c.  The cell's star position and
+// magnitude use the same exact operations as star_layer.
+__device__ __forceinline__ bool cell_star_clear(f3 c, f3 fc, float m, float sharp)
+{
+    const f3 h = hash33(c);
+    const f3 dv = v3(fc.x - (0.10f + 0.80f * h.x), fc.y - (0.10f + 0.80f * h.y), fc.z - (0.10f + 0.80f * h.z));
+    const float dist = sqrtf(dot3(dv, dv));
+    const float mag = hash12(add_x(c.x, mul_x(91.7f, c.z)), sub_x(c.y, mul_x(33.1f, c.x)));
+    const float cut = (mag > 0.9f) ? 60.f : 14.f;
+    return dist - m > sqrtf(cut / sharp);
+}
+
 // Is one star lattice (trace.cuh:131-164: `cell` cells per unit direction, one
-// candidate star per cell, drawn only inside its own cell and only where
-// d2 * sharp <= cut) free of stars everywhere within `r` of the direction d?
-// True when the whole disc stays inside d's cell (all cell faces farther than
-// the margin) and the cell's star, cut radius included, lies beyond it.  The
-// cell and star position use the same exact operations as star_layer.
+// candidate star per cell, drawn only inside its own cell) free of stars
+// everywhere within `r` of the direction d?  Every cell the disc reaches is
+// checked: d's own cell and, along each axis whose face lies within the
+// margin, the neighbouring cell (up to 8 cells at a corner).  A disc wider than
+// half a cell is not cleared.
 __device__ __forceinline__ bool star_layer_clear(f3 d, float cell, float sharp, float r)
 {
     const f3 p = v3(mul_x(d.x, cell), mul_x(d.y, cell), mul_x(d.z, cell));
     const f3 id = v3(floorf(p.x), floorf(p.y), floorf(p.z));
     const f3 f = v3(sub_x(p.x, id.x), sub_x(p.y, id.y), sub_x(p.z, id.z));
     const float m = 1.5f * r * cell + 1e-5f;     // the offsets reach sqrt(2) r; margin in cell units
-    const float face = fminf(fminf(fminf(f.x, 1.f - f.x), fminf(f.y, 1.f - f.y)), fminf(f.z, 1.f - f.z));
-    if (face <= m) return false;
-    const f3 h = hash33(id);
-    const f3 dv = v3(f.x - (0.10f + 0.80f * h.x), f.y - (0.10f + 0.80f * h.y), f.z - (0.10f + 0.80f * h.z));
-    const float dist = sqrtf(dot3(dv, dv));
-    const float mag = hash12(add_x(id.x, mul_x(91.7f, id.z)), sub_x(id.y, mul_x(33.1f, id.x)));
-    const float cut = (mag > 0.9f) ? 60.f : 14.f;
-    return dist - m > sqrtf(cut / sharp);
+    if (m >= 0.5f) return false;
+    const int x0 = f.x < m ? -1 : 0, x1 = f.x > 1.f - m ? 1 : 0;
+    const int y0 = f.y < m ? -1 : 0, y1 = f.y > 1.f - m ? 1 : 0;
+    const int z0 = f.z < m ? -1 : 0, z1 = f.z > 1.f - m ? 1 : 0;
+#pragma unroll 1
+    for (int dz = z0; dz <= z1; ++dz)
+#pragma unroll 1
+        for (int dy = y0; dy <= y1; ++dy)
+#pragma unroll 1
+            for (int dx = x0; dx <= x1; ++dx)
+            {
+                const f3 c = v3(id.x + (float)dx, id.y + (float)dy, id.z + (float)dz);
+                const f3 fc = v3(f.x - (float)dx, f.y - (float)dy, f.z - (float)dz);
+                if (!cell_star_clear(c, fc, m, sharp)) return false;
+            }
+    return true;
 }
 
 // No star of the four lattices of backgroundColor within r of d: the rest of the
