@@ -454,3 +454,28 @@ def test_anchored_frames_accumulate_like_plain_frames(cuda, derive, mode):
         assert np.all(np.isfinite(fb.accum.cpu().numpy()))
     finally:
         net.close()
+
+
+def test_anchored_frame_against_the_reference_and_the_oracle(cuda, derive, oracle):
+    """The anchored frame against the reference's own output, not only against this library's plain
+    frame: the 320x180 Schwarzschild frame of the golden data (the reference's host build) and a
+    480x270 Kerr-Newman orbit frame through the CPU oracle, both at stride 4 without the cell gate,
+    within +-1 LSB on >= 99.9 % of pixels (at 320x180 the hole and disk fill most of the frame: a
+    tenth of the pixels is interpolated; at 480x270 a third)."""
+    import golden_data as G
+    import parity
+    net = Net(5)
+    try:
+        _anchors(net, 4, use_net=0)
+        z = np.load(G.PATH.replace("golden.npz", "config1_schwarzschild_320x180.npz"))
+        cases = [(G.params(z["params"]), z["rgba"], 0.1)]
+        P = _kn_scene(derive, 480, 270, az=75.0)
+        cases.append((P, oracle.pipeline(P)[0], 1.0 / 3.0))
+        for P, want, min_interp in cases:
+            out, _, st = _render(net, P)
+            s = parity.compare_rgba(out, want)
+            print(P.width, P.height, s, "interpolated", int(st[7]))
+            assert s["alpha_ok"] and s["lsb1_frac"] >= 0.999, s
+            assert st[7] > min_interp * P.width * P.height
+    finally:
+        net.close()
