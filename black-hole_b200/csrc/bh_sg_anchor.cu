@@ -243,7 +243,7 @@ __global__ void __launch_bounds__(256, 4) anchor_resolve_kernel(const __grid_con
         float4 v = make_float4(0.f, 0.f, 0.f, 0.f);
         if (ax >= 0 && ay >= 0 && ax < F.nx && ay < F.ny)
         {
-            const BHAnchor& a = F.anchors[F.slot[ay * F.nx + ax]];
+            const BHAnchor& a = F.anchors[ay * F.nx + ax];
             v = make_float4(a.escDir.x, a.escDir.y, a.escDir.z, __uint_as_float(a.flags));
         }
         sAnc[r][c] = v;
@@ -259,7 +259,7 @@ __global__ void __launch_bounds__(256, 4) anchor_resolve_kernel(const __grid_con
         const int cx = x / S, cy = y / S;
         if (x == cx * S && y == cy * S)
         {   // an anchor: its own RK4 sample, unless the anchor pass's step budget ran out
-            const BHAnchor& a = F.anchors[F.slot[cy * F.nx + cx]];
+            const BHAnchor& a = F.anchors[cy * F.nx + cx];
             hdr = v3(a.hdr.x, a.hdr.y, a.hdr.z);
             incomplete = (a.flags & BH_ANCHOR_INCOMPLETE) != 0u;
             anchor = !incomplete;

@@ -135,7 +135,7 @@ struct BHSurrogate
     float epsMax = 1e-4f, maxStep = 0.5f;
     int aW = 0, aH = 0, aS = 0, aNx = 0, aNy = 0;
     unsigned* anchorPix = nullptr;    // anchor pixels in trace order
-    unsigned* anchorSlot = nullptr;   // anchor (ax, ay) -> its index in anchorPix / anchorRec
+    unsigned* anchorRecIdx = nullptr; // trace position k -> the row-major record of anchorPix[k]
     unsigned* blockOrder = nullptr;   // resolve pass: 32 x 8 pixel blocks, nearest the screen centre first
     size_t bCapOrder = 0;
     BHAnchor* anchorRec = nullptr;
@@ -152,7 +152,7 @@ void freeAll(BHSurrogate* s)
     SgState& S = s->S;
     sg_free_batch(S);
     void* ps[] = {S.params, S.grads, S.adamM, S.adamV, S.W, S.Wt, S.biasPacked, S.loss, S.dsIn, S.dsTgt, s->list,
-                  s->counters, s->heldPix, s->heldPred, s->bIn, s->bTgt, s->anchorPix, s->anchorSlot, s->anchorRec,
+                  s->counters, s->heldPix, s->heldPred, s->bIn, s->bTgt, s->anchorPix, s->anchorRecIdx, s->anchorRec,
                   s->cellPix, s->cellGate, s->sampleDir, s->samplePix, s->blockOrder};
     for (void* p : ps)
         if (p) cudaFree(p);
@@ -269,11 +269,11 @@ cudaError_t ensureAnchors(BHSurrogate* s, int W, int H, int S)
     if (nA > s->aCap)
     {
         if (s->anchorPix) cudaFree(s->anchorPix);
-        if (s->anchorSlot) cudaFree(s->anchorSlot);
+        if (s->anchorRecIdx) cudaFree(s->anchorRecIdx);
         if (s->anchorRec) cudaFree(s->anchorRec);
-        s->anchorPix = nullptr; s->anchorSlot = nullptr; s->anchorRec = nullptr; s->aCap = 0;
+        s->anchorPix = nullptr; s->anchorRecIdx = nullptr; s->anchorRec = nullptr; s->aCap = 0;
         if ((e = bh_device_alloc(reinterpret_cast<void**>(&s->anchorPix), nA * sizeof(unsigned)))) return e;
-        if ((e = bh_device_alloc(reinterpret_cast<void**>(&s->anchorSlot), nA * sizeof(unsigned)))) return e;
+        if ((e = bh_device_alloc(reinterpret_cast<void**>(&s->anchorRecIdx), nA * sizeof(unsigned)))) return e;
         if ((e = bh_device_alloc(reinterpret_cast<void**>(&s->anchorRec), nA * sizeof(BHAnchor)))) return e;
         s->aCap = nA;
     }
@@ -296,7 +296,8 @@ cudaError_t ensureAnchors(BHSurrogate* s, int W, int H, int S)
         key[g] = dx * dx + dy * dy;
     }
     std::stable_sort(groups.begin(), groups.end(), [&](unsigned p, unsigned q) { return key[p] < key[q]; });
-    std::vector<unsigned> a, slot(nA), c(nC, 0u);
+    std::vector<unsigned> a, recIdx, c(nC, 0u);
+    recIdx.reserve(nA);
     a.reserve(nA);
     for (unsigned g : groups)
         for (int j = 0; j < 4; ++j)
@@ -304,7 +305,7 @@ cudaError_t ensureAnchors(BHSurrogate* s, int W, int H, int S)
             {
                 const int x = (int)(g % gx) * 8 + i, y = (int)(g / gx) * 4 + j;
                 if (x >= nx || y >= ny) continue;
-                slot[(size_t)y * nx + x] = (unsigned)a.size();
+                recIdx.push_back((unsigned)(y * nx + x));
                 a.push_back((unsigned)(y * S) * (unsigned)W + (unsigned)(x * S));
             }
     for (int y = 0; y + 1 < ny; ++y)
@@ -314,7 +315,7 @@ cudaError_t ensureAnchors(BHSurrogate* s, int W, int H, int S)
     // pageable copies must have landed before a kernel on any stream reads them
     if ((e = cudaDeviceSynchronize())) return e;
     if ((e = cudaMemcpy(s->anchorPix, a.data(), nA * sizeof(unsigned), cudaMemcpyHostToDevice))) return e;
-    if ((e = cudaMemcpy(s->anchorSlot, slot.data(), nA * sizeof(unsigned), cudaMemcpyHostToDevice))) return e;
+    if ((e = cudaMemcpy(s->anchorRecIdx, recIdx.data(), nA * sizeof(unsigned), cudaMemcpyHostToDevice))) return e;
     // resolve blocks (32 x 8 pixels) nearest the screen centre first
     const int rbx = (W + 31) / 32, rby = (H + 7) / 8;
     const size_t nB = (size_t)rbx * rby;
@@ -357,6 +358,7 @@ cudaError_t anchoredFrame(BHSurrogate* s, const RenderParams& P, float4* accum, 
     TraceParams t = bh_frame_params(P, BH_OUT_ANCHOR, s->anchorRec);
     if (s->anchorSteps > 0 && s->anchorSteps < t.maxSteps) t.maxSteps = s->anchorSteps;
     t.pixList = s->anchorPix;
+    t.outIndex = s->anchorRecIdx;     // records land row-major for the resolve pass
     t.nRays = nA;
     if ((e = bh_device_counter(&t.counter)) != cudaSuccess) return e;
     if ((e = bh_launch_trace(t, BH_PREC_FP32, false, bh_family_blocks(P), stream)) != cudaSuccess) return e;
@@ -377,7 +379,6 @@ cudaError_t anchoredFrame(BHSurrogate* s, const RenderParams& P, float4* accum, 
     SgAnchorFrame A{};
     A.tp = bh_frame_params(P, BH_OUT_ACCUM, accum);
     A.anchors = s->anchorRec;
-    A.slot = s->anchorSlot;
     A.blockOrder = s->blockOrder;
     A.S = S; A.nx = s->aNx; A.ny = s->aNy;
     A.cellGate = s->anchorNet ? s->cellGate : nullptr;

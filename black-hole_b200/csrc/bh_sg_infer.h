@@ -52,7 +52,7 @@ cudaError_t sg_infer_launch(const SgInferArgs& a, const SgFrame* frame, cudaStre
 
 // Anchored surrogate frame (bh_sg_anchor.cu).  The anchors are the pixels
 // (S ax, S ay), ax < nx = (W - 1) / S + 1, ay < ny = (H - 1) / S + 1, traced
-// by RK4 into `anchors` (BH_OUT_ANCHOR records, in trace order).  The resolve
+// by RK4 into `anchors` (BH_OUT_ANCHOR records, row-major).  The resolve
 // pass writes every anchor's HDR and every pixel it can interpolate to the
 // accumulation buffer (tp.out), appends the pixels to trace to `list` in
 // whole 8x4 tiles, and records the held-out sample in heldPix.  Pixels whose
@@ -62,8 +62,7 @@ cudaError_t sg_infer_launch(const SgInferArgs& a, const SgFrame* frame, cudaStre
 struct SgAnchorFrame
 {
     TraceParams tp;
-    const BHAnchor* anchors;        // in trace order (8x4 anchor tiles, centre-out)
-    const unsigned* slot;           // anchor (ax, ay) -> its record: slot[ay * nx + ax]
+    const BHAnchor* anchors;        // row-major: anchor (ax, ay) at ay * nx + ax
     const unsigned* blockOrder;     // null, or resolve block k -> 32 x 8 pixel block (row-major index)
     int S, nx, ny;
     const float2* cellGate;         // null, or per cell (nx - 1) x (ny - 1): (P(sky), P(shadow))

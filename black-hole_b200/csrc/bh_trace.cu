@@ -119,7 +119,7 @@ BH_DEV void shade_slot(const TraceParams& P, const PackedRay<typename Ray::Real>
                   ((q.key & kRayExhausted) ? BH_ANCHOR_INCOMPLETE : 0u);
         a.hdr = make_float3(hdr.x, hdr.y, hdr.z);
         a.trans = q.trans;
-        reinterpret_cast<BHAnchor*>(P.out)[key] = a;
+        reinterpret_cast<BHAnchor*>(P.out)[P.outIndex ? __ldg(P.outIndex + key) : key] = a;
         break;
     }
     default:

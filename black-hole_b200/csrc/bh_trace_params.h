@@ -112,6 +112,7 @@ struct TraceParams
     const unsigned* tileOrder;    // non-null: k-th claimed tile -> tile index (trace order)
     const unsigned* pixList;      // non-null: ray k traces pixel pixList[k] (y * W + x)
     const unsigned* nRaysDev;     // non-null: the ray count is read here at kernel start
+    const unsigned* outIndex;     // BH_OUT_ANCHOR, non-null: list position k writes record outIndex[k]
 
     CamFrame<float> cf;           // FP32 integration
     CamFrame<double> cd;          // FP64 integration
