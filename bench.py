@@ -36,7 +36,7 @@ Mrays/s (one primary ray per pixel) over the whole job, and 4K frame ms.
              bhSurrogateRender vs the plain frame in its anchored and network
              forms under the strict acceptance gate (and a permissive one),
              pixels within +-1 LSB; and the default anchored form with two
-             frames in flight (two handles, two streams).
+             frames in flight (the handle and its clone on two streams).
   mixed_precision_4k, batch_256_views, post_process, accuracy, kerr_pair_1080
              (1 GPU; --no-configs skips them) the other workloads: the
              near-extremal 4K elevation sweep (FP32 vs mixed precision, frame
@@ -413,24 +413,20 @@ SG_FRAMES = (0, 50, 100, 150, 200, 250)        # of the 300-frame orbit (azimuth
 
 
 def two_stream_frames(L, h, scene, fa):
-    """The default anchored form with two frames in flight: a second surrogate handle with the same
-    weights renders every other orbit frame on its own stream (the frames of a pair overlap, so one
+    """The default anchored form with two frames in flight: a clone of the handle (same weights and
+    settings, its own scratch) renders every other orbit frame on its own stream (the frames of a pair overlap, so one
     frame's anchor pass and resolve passes fill the other's tails).  frame_ms = a pair's time / 2."""
     import ctypes as C
     import torch
     from bhrt import lib
     from bhrt.device import Frame
     ptr = lambda t: C.c_void_p(t.data_ptr())  # noqa: E731
+    lib.check(L.bhSurrogateSetAnchors(h, 8, 1, C.c_float(1e-4), C.c_float(0.5)), "anchors")
+    lib.check(L.bhSurrogateSetGate(h, C.c_float(0.95), C.c_float(0.95), C.c_float(0.02), 256), "gate")
     h2 = C.c_void_p()
-    lib.check(L.bhSurrogateCreate(C.byref(h2), 7), "bhSurrogateCreate")
+    lib.check(L.bhSurrogateClone(h, C.byref(h2)), "bhSurrogateClone")   # same weights and settings
     try:
-        w = np.zeros(L.bhSurrogateParamCount(), dtype=np.float32)
-        lib.check(L.bhSurrogateGetParams(h, w.ctypes.data_as(C.c_void_p)), "bhSurrogateGetParams")
-        lib.check(L.bhSurrogateSetParams(h2, w.ctypes.data_as(C.c_void_p)), "bhSurrogateSetParams")
         hs = (h, h2)
-        for hh in hs:
-            lib.check(L.bhSurrogateSetAnchors(hh, 8, 1, C.c_float(1e-4), C.c_float(0.5)), "anchors")
-            lib.check(L.bhSurrogateSetGate(hh, C.c_float(0.95), C.c_float(0.95), C.c_float(0.02), 256), "gate")
         fs = (Frame(SG_W, SG_H), Frame(SG_W, SG_H))
         ss = (torch.cuda.Stream(), torch.cuda.Stream())
         cur = torch.cuda.current_stream()

@@ -64,6 +64,7 @@ _SIGNATURES = {
     "bhSurrogateSetGate": (_int, [_vp, C.c_float, C.c_float, C.c_float, _int]),
     "bhSurrogateSetAnchors": (_int, [_vp, _int, _int, C.c_float, C.c_float]),
     "bhSurrogateSetAnchorSteps": (_int, [_vp, _int]),
+    "bhSurrogateClone": (_int, [_vp, _vp]),
     "bhTcWaitProbe": (_int, [_int, _vp]),
     "bhVersion": (C.c_char_p, []),
 }

@@ -487,6 +487,29 @@ cudaError_t bhSurrogateGetParams(BHSurrogate* s, float* host)
     return cudaMemcpy(host, s->S.params, SgLayout::count() * sizeof(float), cudaMemcpyDeviceToHost);
 }
 
+cudaError_t bhSurrogateClone(BHSurrogate* src, BHSurrogate** out)
+{
+    if (!src || !out) return cudaErrorInvalidValue;
+    *out = nullptr;
+    std::vector<float> p((size_t)SgLayout::count());
+    cudaError_t e = bhSurrogateGetParams(src, p.data());
+    if (e != cudaSuccess) return e;
+    BHSurrogate* c = nullptr;
+    if ((e = bhSurrogateCreate(&c, 1u)) != cudaSuccess) return e;
+    if ((e = bhSurrogateSetParams(c, p.data())) != cudaSuccess)
+    {
+        bhSurrogateDestroy(c);
+        return e;
+    }
+    // the frame settings; scratch, statistics and the ray set stay the clone's own
+    c->minProb = src->minProb; c->minConf = src->minConf; c->critBand = src->critBand;
+    c->heldStride = src->heldStride;
+    c->anchorStride = src->anchorStride; c->anchorNet = src->anchorNet;
+    c->epsMax = src->epsMax; c->maxStep = src->maxStep; c->anchorSteps = src->anchorSteps;
+    *out = c;
+    return cudaSuccess;
+}
+
 cudaError_t bhSurrogateSetParams(BHSurrogate* s, const float* host)
 {
     if (!s || !host) return cudaErrorInvalidValue;

@@ -72,6 +72,12 @@ int bhSurrogateParamCount(void);
 cudaError_t bhSurrogateCreate(BHSurrogate** s, unsigned seed);
 void bhSurrogateDestroy(BHSurrogate* s);
 
+/* A second handle with the same parameters and frame settings (form, gate,
+ * anchor stride and budget), its own scratch and statistics and no ray set
+ * (blocking): with the source on one stream and the clone on another, two
+ * frames are rendered at once (frames in flight).  Destroy it on its own. */
+cudaError_t bhSurrogateClone(BHSurrogate* src, BHSurrogate** out);
+
 /* Copy the FP32 parameter vector to / from host memory (blocking); setting
  * parameters resets the optimiser state. */
 cudaError_t bhSurrogateGetParams(BHSurrogate* s, float* host);

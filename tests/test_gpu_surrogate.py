@@ -479,3 +479,28 @@ def test_anchored_frame_against_the_reference_and_the_oracle(cuda, derive, oracl
             assert st[7] > min_interp * P.width * P.height
     finally:
         net.close()
+
+
+def test_clone_renders_the_source_handles_frames(cuda, derive):
+    """bhSurrogateClone: a handle with the source's weights and frame settings (here the anchored
+    form at stride 4 with its network cell gate and no held-out sample) renders the same frame bit
+    for bit, on its own scratch."""
+    net = Net(5)
+    clone = C.c_void_p()
+    try:
+        _anchors(net, 4, use_net=1)
+        assert net.L.bhSurrogateSetGate(net.h, C.c_float(0.3), C.c_float(0.0), C.c_float(0.02), 0) == 0
+        assert net.L.bhSurrogateClone(net.h, C.byref(clone)) == 0
+        P = _kn_scene(derive, 480, 270, az=75.0)
+        out, acc, st = _render(net, P)
+        f = Frame(480, 270)
+        assert net.L.bhSurrogateRender(clone, _ptr(f.out), _ptr(f.accum), _ptr(f.bloomA), _ptr(f.bloomB),
+                                       C.byref(P), _stream()) == 0
+        st2 = np.zeros(16, dtype=np.uint32)
+        assert net.L.bhSurrogateFrameStats(clone, st2.ctypes.data_as(C.c_void_p)) == 0
+        assert np.array_equal(f.accum.cpu().numpy(), acc) and np.array_equal(f.out.cpu().numpy(), out)
+        assert np.array_equal(st2, st) and st[6] == 120 * 68
+    finally:
+        if clone.value:
+            net.L.bhSurrogateDestroy(clone)
+        net.close()
