@@ -527,3 +527,20 @@ def test_anchored_frames_on_random_views(cuda, derive):
             assert np.array_equal(acc[::8, ::8], pacc[::8, ::8]) or st[12] > 0   # anchors (unless re-traced)
     finally:
         net.close()
+
+
+@pytest.mark.parametrize("w,h", [(1, 1), (7, 3), (9, 9), (17, 10), (33, 2)])
+def test_anchored_frame_tiny_sizes_equal_plain(cuda, derive, w, h):
+    """Frames smaller than a 4x4 anchor stencil: every pixel is an anchor or traced, so the anchored
+    frame is the plain frame bit for bit (edge handling of the anchor lattice, the resolve blocks and
+    the padded list tiles)."""
+    net = Net(5)
+    try:
+        _anchors(net, 8, use_net=0)
+        P = _kn_scene(derive, w, h, az=75.0)
+        out, acc, st = _render(net, P)
+        pout, pacc = _plain(P)
+        assert st[7] == 0 and st[0] == w * h
+        assert np.array_equal(acc, pacc) and np.array_equal(out, pout)
+    finally:
+        net.close()
