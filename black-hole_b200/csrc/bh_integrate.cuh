@@ -560,44 +560,14 @@ BH_DEV void kerr_rk4(const CamFrame<S>& F, const KerrConsts<V>& k, V h, V& r, V&
     ph = vfma(h6, vfma(iS4, d4.ph, sph), ph);
 }
 
-// One RK4 step of the Kerr-Newman system in FP64 from an FP32 state (the
-// right-hand side at the start is re-evaluated in FP64).  Out of line so the
-// FP32 step loop keeps its register budget.
-struct KerrStep64 { float r, th, ph, pr, pth, dr4, dth4, dph4; };
-
-static __device__ __noinline__ KerrStep64 kerr_rk4_fp64(const CamFrame<double>& F, float Ef, float Lzf, float r0,
-                                                        float th0, float ph0, float pr0, float pth0, float hf)
-{
-    const double E = Ef, Lz = Lzf, h = hf;
-    const KerrConsts<double> k{E, Lz, F.a * E, E * F.a2 - F.a * Lz, 2.0 * E};
-    double r = r0, th = th0, ph = ph0, pr = pr0, pth = pth0, s, c;
-    sincos(th, &s, &c);
-    KerrDeriv<double> d1 = kerr_rhs(F, k, r, s, c, pr, pth).d;
-    const double hh = 0.5 * h;
-    sincos(th + hh * d1.th, &s, &c);
-    KerrDeriv<double> d2 = kerr_rhs(F, k, r + hh * d1.r, s, c, pr + hh * d1.pr, pth + hh * d1.pth).d;
-    sincos(th + hh * d2.th, &s, &c);
-    KerrDeriv<double> d3 = kerr_rhs(F, k, r + hh * d2.r, s, c, pr + hh * d2.pr, pth + hh * d2.pth).d;
-    sincos(th + h * d3.th, &s, &c);
-    KerrDeriv<double> d4 = kerr_rhs(F, k, r + h * d3.r, s, c, pr + h * d3.pr, pth + h * d3.pth).d;
-    const double h6 = h / 6.0;
-    KerrStep64 o;
-    o.r = (float)(r + h6 * (d1.r + 2.0 * d2.r + 2.0 * d3.r + d4.r));
-    o.th = (float)(th + h6 * (d1.th + 2.0 * d2.th + 2.0 * d3.th + d4.th));
-    o.ph = (float)(ph + h6 * (d1.ph + 2.0 * d2.ph + 2.0 * d3.ph + d4.ph));
-    o.pr = (float)(pr + h6 * (d1.pr + 2.0 * d2.pr + 2.0 * d3.pr + d4.pr));
-    o.pth = (float)(pth + h6 * (d1.pth + 2.0 * d2.pth + 2.0 * d3.pth + d4.pth));
-    o.dr4 = (float)d4.r; o.dth4 = (float)d4.th; o.dph4 = (float)d4.ph;
-    return o;
-}
-
 // MIXED: FP32 state and steps; FP64 initial data (tetrad map and camera
-// position), whole steps in FP64 at radial turning points (p_r would change
-// sign within the step -- for near-extremal holes this includes periapses a
-// few percent outside the horizon), FP64 state and steps through every polar
-// passage (|sin th| < kPolarCap, below), and FP64 bisection of the equatorial
-// crossing.  (FP64 steps over the whole final horizon approach were measured
-// to cost 70 % more time for no accuracy gain, and are not taken.)
+// position), FP64 state and steps through every polar passage (|sin th| <
+// kPolarCap, below), and FP64 bisection of the equatorial crossing.  (Not
+// taken, measured on the near-extremal 4K sweep against the all-FP64
+// integration: FP64 steps over the whole final horizon approach, 70 % more
+// time for no accuracy gain; FP64 steps at radial turning points, where p_r
+// would change sign within the step, 23 % more time for the same accuracy to
+// five digits at every elevation.)
 //
 // Polar passages.  A ray that passes within a small angle th_min of the spin
 // axis swings its azimuth by ~pi and reverses p_th within a few steps, and the
@@ -735,17 +705,9 @@ struct KerrRay
         h = min_p(h, capLen * rcp_p(spd));
 
         const R rS = r, thS = th, drS = d1.r, dthS = d1.th;    // step start (crossing search)
-        R dl0 = R(0), dl1 = R(0), dl2 = R(0);                 // the final stage's derivative
         if constexpr (MIXED)
         {
             if (abs_p(s) < R(kPolarCap)) return polar_passage_fp64(P);
-            if (abs_p(pr) < h * abs_p(d1.pr))
-            {
-                KerrStep64 o = kerr_rk4_fp64(P.cd, k.E, k.Lz, r, th, ph, pr, pth, h);
-                r = o.r; th = o.th; ph = o.ph; pr = o.pr; pth = o.pth;
-                dl0 = o.dr4; dl1 = o.dth4; dl2 = o.dph4;
-                return finish_step(P, F, h, rS, thS, drS, dthS, dl0, dl1, dl2, R(1));
-            }
         }
 
         KerrDeriv<R> d4;

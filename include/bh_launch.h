@@ -38,8 +38,10 @@ enum { BH_SCHWARZSCHILD = 0, BH_REISSNER_NORDSTROM = 1, BH_KERR = 2, BH_KERR_NEW
 /* Arithmetic of the geodesic integration.
  *  BH_PREC_FP32  : everything in FP32 (the reference's arithmetic).
  *  BH_PREC_MIXED : FP32 stepping; FP64 for the conserved-quantity set-up at
- *                  the camera, for the horizon/turning-point and escape
- *                  decisions, and for bisection of equatorial disk crossings.
+ *                  the camera, for every passage of the Kerr-family polar cap
+ *                  (|sin th| < 1/64, state carried in FP64), for the
+ *                  spherical family's turning-point steps, and for bisection
+ *                  of equatorial disk crossings.
  *  BH_PREC_FP64  : the whole integration in FP64 (GPU oracle). */
 enum { BH_PREC_FP32 = 0, BH_PREC_MIXED = 1, BH_PREC_FP64 = 2 };
 
